@@ -1,0 +1,171 @@
+/*
+ * simpfem: B200-native guarded SIMP-floor linear-elasticity solve (C ABI).
+ *
+ * Every entry point returns 0 on success or a positive SIMPFEM_E* status; the
+ * message of the last failure on the calling thread is simpfem_last_error().
+ * Array arguments are device pointers unless the name ends in _host.  "free"
+ * vectors are the reference's compact free-DOF vectors (length n_free, in the
+ * order of the free-DOF list given to simpfem_mesh_create); "full" vectors have
+ * one entry per global DOF (3 * n_nodes) and hold 0 at constrained DOFs.
+ * Streams are cudaStream_t passed as void* (NULL = legacy default stream).  No
+ * call allocates caller-visible memory; a handle keeps its own work buffers.
+ * Element moduli E are indexed e = (i * nely + j) * nelz + k as in the
+ * reference (gpu_fem/pub_simp_solver.py:196-207).
+ */
+#ifndef SIMPFEM_H
+#define SIMPFEM_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SIMPFEM_OK = 0,
+  SIMPFEM_EINVAL = 1,       /* bad argument */
+  SIMPFEM_ECUDA = 2,        /* CUDA runtime failure */
+  SIMPFEM_ENOTSETUP = 5,    /* apply before setup (reference raises RuntimeError) */
+  SIMPFEM_ENONFINITE = 6,   /* non-finite input or result */
+  SIMPFEM_EINTERNAL = 9
+};
+
+enum { SIMPFEM_F64 = 0, SIMPFEM_F32 = 1, SIMPFEM_BF16 = 2 };
+
+typedef struct simpfem_mesh simpfem_mesh;
+typedef struct simpfem_gmg simpfem_gmg;
+
+const char* simpfem_last_error(void);
+int simpfem_version(void);
+
+/* Structured hex8 mesh of nelx*nely*nelz unit elements with the given free-DOF
+ * list (ascending global DOF indices) and the 24x24 unit element stiffness in
+ * the reference's local order.  Replaces the state MatrixFreeKff.__init__ keeps
+ * (gpu_fem/solver_v2.py:1153-1176); the edof table is implicit. */
+int simpfem_mesh_create(int nelx, int nely, int nelz, const int32_t* free_dofs_host,
+                        int64_t n_free, const double* ke_unit_host, simpfem_mesh** out);
+int simpfem_mesh_destroy(simpfem_mesh* m);
+int simpfem_mesh_info(const simpfem_mesh* m, int64_t* ndof, int64_t* n_free, int64_t* n_elem);
+/* Pick the sweep tile shape of the fine operator by timing candidates (the tuner);
+ * runs on first use otherwise. */
+int simpfem_mesh_tune(simpfem_mesh* m, void* stream);
+
+/* y_free = K_ff(E) u_free; dtype SIMPFEM_F64 or SIMPFEM_F32 for E/u/y
+ * (MatrixFreeKff.matvec, gpu_fem/solver_v2.py:1182-1222). */
+int simpfem_matvec(simpfem_mesh* m, int dtype, const void* E, const void* u_free, void* y_free,
+                   void* stream);
+/* Full-layout operator (FusedMatvec.matvec_full, gpu_fem/cuda_fused_matvec.py:379-391):
+ * dtype SIMPFEM_F32 or SIMPFEM_BF16 (bf16-rounded operands, FP32 accumulation), or F64. */
+int simpfem_matvec_full(simpfem_mesh* m, int dtype, const void* E, const void* u_full,
+                        void* y_full, void* stream);
+/* diag(K_ff) (MatrixFreeKff.extract_diagonal, gpu_fem/solver_v2.py:1228-1251). */
+int simpfem_extract_diagonal(simpfem_mesh* m, const double* E, double* diag_free, void* stream);
+/* 3x3 node-block Jacobi: update with E and the scalar diagonal (free layout, may be
+ * NULL), then apply z = M^{-1} r (NodeBlockJacobiMF.update/apply,
+ * gpu_fem/solver_v2.py:1381-1451).  blocks: n_nodes * 9 doubles owned by the caller. */
+int simpfem_node_blocks(simpfem_mesh* m, const double* E, const double* scalar_diag_free,
+                        double* blocks, void* stream);
+int simpfem_node_block_apply(simpfem_mesh* m, const double* blocks, const double* r_free,
+                             double* z_free, void* stream);
+/* u_e^T KE u_e per element from a free-layout displacement (SolverV4 sensitivity,
+ * gpu_fem/solver_v4.py:257-264). */
+int simpfem_element_energy(simpfem_mesh* m, const double* u_free, double* ce, void* stream);
+/* ||b - K(E) x|| / ||b|| in FP64, written to *out_host (the recomputed true-residual
+ * guard, experiments/phase5/run_gmg_floor_detector_prospective.py:246-247). */
+int simpfem_true_residual(simpfem_mesh* m, const double* E, const double* b_free,
+                          const double* x_free, double* out_host, void* stream);
+
+/* Options of the Galerkin GMG hierarchy: the keyword arguments of
+ * GalerkinMatFreeGMG.__init__ (gpu_fem/multigrid_v4.py:546-580).  The caller
+ * validates them (the Python layer raises the reference's ValueErrors). */
+typedef struct simpfem_gmg_opts {
+  int n_levels;                    /* 4 */
+  int coarse_smooth_iters;         /* 2 */
+  int fine_smoother;               /* SIMPFEM_F64 / F32 / BF16 ("fp64","fp32","bf16") */
+  int fine_smoother_degree;        /* 2 */
+  double omega;                    /* 0.5 */
+  int dense_chol_max;              /* 5000 */
+  int coarse_pcg_iters;            /* 80 */
+  int smoother_type;               /* 0 chebyshev, 1 jacobi */
+  double cheb_lower_frac;          /* 1/30 */
+  int level_prec[8];               /* per level dtype; -1 = reference default schedule */
+  int cycle_type;                  /* 0 V, 1 W */
+  int coarse_correction_policy;    /* 0 none, 1 residual_line_search */
+  double coarse_correction_acceptance_ratio; /* 1.0 */
+  double coarse_correction_max_scale;        /* 1.0 */
+  int root_enrichment_mode;        /* 0 none, 1 weighted_residual_second, 2 weighted_gap_second,
+                                      3 void_residual_second, 4 void_gap_second */
+  double root_enrichment_weight_floor;  /* 1e-6 */
+  double root_enrichment_weight_power;  /* 0.5 */
+  int root_local_correction_mode;  /* 0 none, 1 node_block_line_search, 2 node_block_inner_fgmres */
+  double root_local_correction_max_scale; /* 1.0 */
+  int root_local_correction_inner_steps;   /* 10 */
+  int root_local_correction_inner_restart; /* steps when <= 0 */
+  int inner_krylov_steps;          /* 0 */
+  int inner_krylov_restart;        /* steps when <= 0 */
+  int cycle_precision;             /* SIMPFEM_F64: the reference's FP64 cycle with per-level
+                                      smoother precision; SIMPFEM_F32: mixed mode, the whole
+                                      V-cycle in FP32 with BF16-stored coarse stencils
+                                      (no reference counterpart) */
+  int use_graphs;                  /* capture the preconditioner apply in a CUDA graph */
+} simpfem_gmg_opts;
+
+void simpfem_gmg_default_opts(simpfem_gmg_opts* o);
+
+/* Read-only state after setup (GalerkinMatFreeGMG properties, multigrid_v4.py:772-837). */
+typedef struct simpfem_gmg_props {
+  int n_levels;
+  int64_t n_free[8];
+  int dims[8][3];
+  double lambda_max[8];
+  double omega_used;
+  double contrast_ratio;
+  double void_fraction;
+  int is_high_contrast;
+  int fine_degree_adapt;
+  int coarse_iters_adapt;
+  int level_prec[8];
+  int coarse_mode;          /* 0 none, 1 dense Cholesky, 2 iterative (fixed Jacobi-PCG) */
+  int coarse_regularised;   /* 1 if the eps-regularised retry was used */
+  int lambda_reestimated;   /* 1 if the last setup re-estimated lambda_max */
+  int64_t nnz[8];           /* structural nonzeros of the coarse operators (free-free) */
+} simpfem_gmg_props;
+
+int simpfem_gmg_create(simpfem_mesh* m, const simpfem_gmg_opts* opts, simpfem_gmg** out);
+int simpfem_gmg_destroy(simpfem_gmg* g);
+/* GalerkinMatFreeGMG.setup (multigrid_v4.py:1119-1341); fine_diag_free may be NULL. */
+int simpfem_gmg_setup(simpfem_gmg* g, const double* E, const double* fine_diag_free, void* stream);
+/* z = M(rhs) (GalerkinMatFreeGMG.apply, multigrid_v4.py:1759-1767); FP64 free layout. */
+int simpfem_gmg_apply(simpfem_gmg* g, const double* rhs_free, double* z_free, void* stream);
+int simpfem_gmg_props_get(simpfem_gmg* g, simpfem_gmg_props* out);
+/* Forget the cached lambda_max estimates (the next setup re-estimates). */
+int simpfem_gmg_reset_lambda_cache(simpfem_gmg* g);
+/* Copy the fine-level operator of the last setup: E as FP64 (n_elem). */
+int simpfem_gmg_fine_E(simpfem_gmg* g, const double** E_out);
+
+/* FGMRES with the hierarchy as right preconditioner and the fine FP64 operator of
+ * the last setup (_cupy_fgmres, multigrid_v4.py:416-534).  x0_free may be NULL.
+ * history_host receives ||r||/||b|| entries with the reference's rule (start of each
+ * restart, then after every iteration); *history_len may exceed history_cap, in which
+ * case only history_cap entries are written. */
+int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
+                   double tol, int maxiter, int restart, double* history_host, int history_cap,
+                   int* history_len, int* iters, int* converged, void* stream);
+/* PCG with the hierarchy as preconditioner (_cupy_pcg, gpu_fem/solver_v2.py:551-623). */
+int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
+                double tol, int maxiter, double* history_host, int history_cap, int* history_len,
+                int* iters, int* converged, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* SIMPFEM_H */

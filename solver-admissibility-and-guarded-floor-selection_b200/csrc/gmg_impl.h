@@ -1,0 +1,222 @@
+// Host-side structures of the simpfem library shared by gmg.cu and capi.cu.
+#pragma once
+
+#include <math.h>
+
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "simpfem.h"
+
+namespace simpfem {
+
+struct NotSetup {
+  std::string msg;
+};
+
+struct InvalidArg {
+  std::string msg;
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+    o.p = nullptr;
+    o.bytes = 0;
+  }
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void* alloc(size_t b) {
+    if (b == 0) b = 16;
+    if (b <= bytes && p) return p;
+    release();
+    SF_CUDA(cudaMalloc(&p, b));
+    bytes = b;
+    return p;
+  }
+  template <class T>
+  T* as() const { return (T*)p; }
+};
+
+struct PinnedBuf {
+  void* h = nullptr;
+  void* d = nullptr;
+  size_t bytes = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  ~PinnedBuf() {
+    if (h) cudaFreeHost(h);
+  }
+  void alloc(size_t b) {
+    if (b <= bytes && h) return;
+    if (h) cudaFreeHost(h);
+    SF_CUDA(cudaHostAlloc(&h, b, cudaHostAllocMapped));
+    SF_CUDA(cudaHostGetDevicePointer(&d, h, 0));
+    std::memset(h, 0, b);
+    bytes = b;
+  }
+};
+
+struct Mesh {
+  Grid g;
+  int64_t n_free = 0;
+  std::vector<int32_t> free_h;
+  std::vector<uint8_t> mask_h;
+  DevBuf free_idx, mask;
+  double ke[576];
+  WhtBlocks wb;
+  std::vector<double> Q;
+  SweepShape sh[2];
+  bool tuned[2] = {false, false};
+  DevBuf ufull, yfull, scratch;
+  DevBuf red_part, red_ticket;
+  RedWork rw{};
+  DevBuf dscal;  // device scalars
+  int device = 0;
+
+  void init_red() {
+    red_part.alloc(sizeof(double) * 4 * kRedBlocksHost);
+    red_ticket.alloc(sizeof(unsigned) * 4);
+    SF_CUDA(cudaMemset(red_ticket.p, 0, sizeof(unsigned) * 4));
+    rw.partials = red_part.as<double>();
+    rw.ticket = red_ticket.as<unsigned>();
+    dscal.alloc(sizeof(double) * 64);
+  }
+};
+
+struct KrylovWs {
+  int restart = 0;
+  int64_t n = 0;
+  DevBuf V, Z, w, r, H, cs, sn, g, y, sc, Zptr;
+  DevBuf flags_dev;     // device-side control flags (read by every guarded kernel)
+  PinnedBuf flags_pin;  // host mirror, refreshed by sync_flags()
+  KrylovDev kd;
+
+  void ensure(int64_t n_, int restart_) {
+    if (restart_ == restart && n_ == n && V.p) return;
+    restart = restart_;
+    n = n_;
+    V.alloc(sizeof(double) * (size_t)(restart + 1) * n);
+    Z.alloc(sizeof(double) * (size_t)restart * n);
+    w.alloc(sizeof(double) * n);
+    r.alloc(sizeof(double) * n);
+    H.alloc(sizeof(double) * (size_t)(restart + 1) * restart);
+    SF_CUDA(cudaMemset(H.p, 0, sizeof(double) * (size_t)(restart + 1) * restart));
+    cs.alloc(sizeof(double) * restart);
+    sn.alloc(sizeof(double) * restart);
+    g.alloc(sizeof(double) * (restart + 1));
+    y.alloc(sizeof(double) * restart);
+    sc.alloc(sizeof(double) * 16);
+    flags_dev.alloc(sizeof(int) * NFLAGS);
+    SF_CUDA(cudaMemset(flags_dev.p, 0, sizeof(int) * NFLAGS));
+    flags_pin.alloc(sizeof(int) * NFLAGS);
+    std::vector<double*> zp(restart);
+    for (int j = 0; j < restart; ++j) zp[j] = Z.as<double>() + (size_t)j * n;
+    Zptr.alloc(sizeof(double*) * restart);
+    SF_CUDA(cudaMemcpy(Zptr.p, zp.data(), sizeof(double*) * restart, cudaMemcpyHostToDevice));
+    kd.H = H.as<double>();
+    kd.cs = cs.as<double>();
+    kd.sn = sn.as<double>();
+    kd.g = g.as<double>();
+    kd.y = y.as<double>();
+    kd.sc = sc.as<double>();
+    kd.flags = flags_dev.as<int>();
+    kd.restart = restart;
+  }
+  double* Vj(int j) { return V.as<double>() + (size_t)j * n; }
+  double* Zj(int j) { return Z.as<double>() + (size_t)j * n; }
+  const int* hflags() const { return (const int*)flags_pin.h; }
+  void sync_flags(cudaStream_t s) {
+    SF_CUDA(cudaMemcpyAsync(flags_pin.h, flags_dev.p, sizeof(int) * NFLAGS, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+  }
+  const int* dflag(int f) const { return kd.flags + f; }
+};
+
+struct Level {
+  Grid g;
+  std::vector<uint8_t> mask_h;
+  DevBuf mask;
+  int64_t n_free = 0;
+  // transfer weights between this level (fine side) and the next coarser one
+  DevBuf wx, wy, wz;
+  // coarse operator (levels >= 1)
+  DevBuf K64, K32, K16;
+  DevBuf dinv64, dinv32;
+  double lam = NAN;
+  // cycle vectors in the cycle dtype
+  DevBuf x[2], res, c, Ac, d, rhs, trial, res2, ptmp;
+  // FP32 smoothing scratch (reference mode with an fp32 level)
+  DevBuf xs[2], ds, rhss;
+};
+
+struct Gmg {
+  Mesh* m = nullptr;
+  simpfem_gmg_opts o;
+  int L = 1;
+  std::vector<Level> lv;
+  DType cyc = F64;  // cycle vector dtype
+  int prec[8];      // resolved per-level smoother precision
+  bool prec_resolved = false;
+
+  DevBuf E64, E32, diag0, wenrich, binv;
+  bool is_setup = false;
+
+  // lambda cache
+  double lam_Emax = NAN;
+  int lam_calls = 0;
+  bool lam_reest = false;
+  double omega_used;
+  double contrast = NAN, void_frac = 0.0;
+  bool high = false;
+  int fine_deg = 2, coarse_iters = 2;
+
+  // coarsest dense solve
+  int coarse_mode = 0;
+  bool coarse_reg = false;
+  int nc = 0;
+  DevBuf c_idx, c_didx, Adense, Linv, cb, cx, ctmp, cinfo;
+  // iterative coarse (fixed PCG) vectors
+  DevBuf pr, pz, pp, pAp;
+
+  DevBuf sc;         // scalar scratch of the corrections
+  DevBuf rhs64, out64, tmp64a, tmp64b, tmp64c, tmp64d;  // apply-level FP64 vectors
+  DevBuf cyc_in, cyc_out;  // mixed mode: FP32 copies at the cycle boundary
+  KrylovWs ik, rl, outer;
+  cudaStream_t st = nullptr;
+  const int* guard = nullptr;
+
+  // outer solve history (device) and its host copy
+  DevBuf hist_dev;
+  PinnedBuf hist_pin;
+
+  int64_t nfull() const { return m->g.ndof; }
+};
+
+using PrecFn = std::function<void(const double* in, double* out, const int* guard)>;
+
+WhtBlocks make_wht_blocks(const double* ke, double* max_off);
+std::vector<double> make_level1_Q(const double* ke);
+SweepShape default_shape(const Grid& g, int maxt);
+void fine_apply(Mesh& m, DType t, Epi epi, const void* E, const void* u, const EpiArgs& ea, cudaStream_t s);
+void tune_mesh(Mesh& m, DType t, cudaStream_t s);
+Gmg* gmg_create(Mesh* m, const simpfem_gmg_opts& o);
+void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free);
+void apply_full(Gmg& G, const double* rhs, double* out, const int* guard);
+void run_outer_fgmres(Gmg& G, const double* b, double* x, bool x0_zero, double tol, int maxiter, int restart,
+                      const PrecFn& M, double* hist_dev, int hist_cap);
+void run_pcg(Gmg& G, const double* b, double* x, double tol, int maxiter, std::vector<double>* hist, int* iters,
+             int* conv);
+
+}  // namespace simpfem

@@ -1,0 +1,1035 @@
+// Vector, reduction, dense and Krylov kernels of the simpfem library.
+//
+// Reductions are deterministic: a fixed grid writes one partial per block and
+// the last block to finish (ticket counter) sums the partials in block order,
+// so every dot product is bitwise reproducible run to run.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace simpfem {
+
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum of up to 4 values (result valid in thread 0).
+template <int ND>
+__device__ __forceinline__ void block_sum(double (&v)[ND], double* sh /*32*ND*/) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    const double w = warp_sum(v[k]);
+    if (lane == 0) sh[k * 32 + wid] = w;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+      double w = lane < nw ? sh[k * 32 + lane] : 0.0;
+      v[k] = warp_sum(w);
+    }
+  }
+}
+
+// Finalisation by the last block: out[k] = sum of partials in block order.
+template <int ND>
+__device__ __forceinline__ bool last_block_finalize(const double (&v)[ND], RedWork w, double* out) {
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < ND; ++k) w.partials[k * kRedBlocks + blockIdx.x] = v[k];
+    __threadfence();
+    const unsigned t = atomicAdd(w.ticket, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  if (threadIdx.x < ND) {
+    __threadfence();
+    const int k = threadIdx.x;
+    double s = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += ((volatile double*)w.partials)[k * kRedBlocks + b];
+    out[k] = s;
+  }
+  if (threadIdx.x == 0) *w.ticket = 0u;
+  return true;
+}
+
+template <typename T>
+__device__ __forceinline__ double dot_term(const DotSet& ds, int k, int64_t i) {
+  const T a = ((const T*)ds.a[k])[i];
+  const T b = ((const T*)ds.b[k])[i];
+  if (ds.mode[k] == 0) return (double)a * (double)b;
+  const T c = ((const T*)ds.c[k])[i];
+  if (ds.mode[k] == 1) return (double)mul_rn(a, c) * (double)b;  // (a * c) * b
+  // mode 2: a * (b / c) on entries with c != 0
+  return c != T(0) ? (double)a * (double)(b / c) : 0.0;
+}
+
+template <typename T, int ND>
+__global__ void __launch_bounds__(kRedThreads) dots_kernel(int64_t n, DotSet ds, RedWork w, double* out,
+                                                           const int* guard) {
+  if (guard_off(guard)) return;
+  __shared__ double sh[32 * 4];
+  double v[ND];
+#pragma unroll
+  for (int k = 0; k < ND; ++k) v[k] = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+#pragma unroll
+    for (int k = 0; k < ND; ++k) v[k] += dot_term<T>(ds, k, i);
+  }
+  block_sum<ND>(v, sh);
+  last_block_finalize<ND>(v, w, out);
+}
+
+static int red_blocks(int64_t n) {
+  const int64_t b = (n + kRedThreads - 1) / kRedThreads;
+  return (int)(b < kRedBlocks ? (b < 1 ? 1 : b) : kRedBlocks);
+}
+
+cudaError_t launch_dots(DType t, int64_t n, const DotSet& ds, RedWork w, double* out,
+                        const int* guard, cudaStream_t s) {
+  const int nb = red_blocks(n);
+#define SF_DOTS(T)                                                                                 \
+  switch (ds.nd) {                                                                                 \
+    case 1: dots_kernel<T, 1><<<nb, kRedThreads, 0, s>>>(n, ds, w, out, guard); break;            \
+    case 2: dots_kernel<T, 2><<<nb, kRedThreads, 0, s>>>(n, ds, w, out, guard); break;            \
+    case 3: dots_kernel<T, 3><<<nb, kRedThreads, 0, s>>>(n, ds, w, out, guard); break;            \
+    case 4: dots_kernel<T, 4><<<nb, kRedThreads, 0, s>>>(n, ds, w, out, guard); break;            \
+    default: return cudaErrorInvalidValue;                                                         \
+  }
+  if (t == F64) {
+    SF_DOTS(double)
+  } else if (t == F32) {
+    SF_DOTS(float)
+  } else {
+    return cudaErrorInvalidValue;
+  }
+#undef SF_DOTS
+  return cudaGetLastError();
+}
+
+// min, max and count(E > thr) of a double array (contrast classification,
+// gpu_fem/multigrid_v4.py:1204-1239).
+__global__ void __launch_bounds__(kRedThreads) minmax_kernel(int64_t n, const double* __restrict__ E,
+                                                             double thr, RedWork w, double* out) {
+  __shared__ double sh[32 * 3];
+  double v[3] = {INFINITY, -INFINITY, 0.0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double e = E[i];
+    v[0] = fmin(v[0], e);
+    v[1] = fmax(v[1], e);
+    v[2] += (e > thr) ? 1.0 : 0.0;
+  }
+  // min/max reduce via shuffles
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] = fmin(v[0], __shfl_down_sync(0xffffffffu, v[0], o));
+    v[1] = fmax(v[1], __shfl_down_sync(0xffffffffu, v[1], o));
+    v[2] += __shfl_down_sync(0xffffffffu, v[2], o);
+  }
+  if (lane == 0) {
+    sh[wid] = v[0];
+    sh[32 + wid] = v[1];
+    sh[64 + wid] = v[2];
+  }
+  __syncthreads();
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    double a = INFINITY, b = -INFINITY, c = 0.0;
+    for (int k = 0; k < nw; ++k) {
+      a = fmin(a, sh[k]);
+      b = fmax(b, sh[32 + k]);
+      c += sh[64 + k];
+    }
+    w.partials[blockIdx.x] = a;
+    w.partials[kRedBlocks + blockIdx.x] = b;
+    w.partials[2 * kRedBlocks + blockIdx.x] = c;
+    __threadfence();
+    is_last = atomicAdd(w.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (is_last && threadIdx.x == 0) {
+    __threadfence();
+    double a = INFINITY, b = -INFINITY, c = 0.0;
+    volatile double* p = w.partials;
+    for (int k = 0; k < (int)gridDim.x; ++k) {
+      a = fmin(a, p[k]);
+      b = fmax(b, p[kRedBlocks + k]);
+      c += p[2 * kRedBlocks + k];
+    }
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+    *w.ticket = 0u;
+  }
+}
+
+cudaError_t launch_minmax_count(int64_t n, const double* E, double thr, RedWork w, double* out3,
+                                cudaStream_t s) {
+  minmax_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(n, E, thr, w, out3);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Elementwise kernels.
+template <typename T>
+__global__ void axpby_kernel(int64_t n, T alpha, const T* __restrict__ x, T beta, const T* __restrict__ y,
+                             T* __restrict__ out, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  // out = alpha * x + beta * y, each product rounded (numpy semantics); a null
+  // y means out = alpha * x, alpha == 1 skips the product.
+  T a = alpha == T(1) ? x[i] : mul_rn(alpha, x[i]);
+  if (y == nullptr) {
+    out[i] = a;
+    return;
+  }
+  T b = beta == T(1) ? y[i] : (beta == T(-1) ? -y[i] : mul_rn(beta, y[i]));
+  out[i] = add_rn(a, b);
+}
+
+cudaError_t launch_axpby(DType t, int64_t n, double alpha, const void* x, double beta,
+                         const void* y, void* out, const int* guard, cudaStream_t s) {
+  const int nb = div_up(n, 256);
+  if (t == F64)
+    axpby_kernel<double><<<nb, 256, 0, s>>>(n, alpha, (const double*)x, beta, (const double*)y,
+                                            (double*)out, guard);
+  else
+    axpby_kernel<float><<<nb, 256, 0, s>>>(n, (float)alpha, (const float*)x, (float)beta,
+                                           (const float*)y, (float*)out, guard);
+  return cudaGetLastError();
+}
+
+template <typename T>
+__global__ void fill_kernel(int64_t n, T v, T* __restrict__ out, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = v;
+}
+
+cudaError_t launch_fill(DType t, int64_t n, double v, void* out, const int* guard, cudaStream_t s) {
+  const int nb = div_up(n, 256);
+  if (t == F64)
+    fill_kernel<double><<<nb, 256, 0, s>>>(n, v, (double*)out, guard);
+  else
+    fill_kernel<float><<<nb, 256, 0, s>>>(n, (float)v, (float*)out, guard);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy(DType t, int64_t n, const void* src, void* dst, const int* guard,
+                        cudaStream_t s) {
+  return launch_axpby(t, n, 1.0, src, 0.0, nullptr, dst, guard, s);
+}
+
+// First Chebyshev step from x0 = 0 (gpu_fem/multigrid_v4.py:1783-1812 with
+// A(0) = 0): d = dinv * rhs; x = alpha * d.
+template <typename T>
+__global__ void cheb_zero_kernel(int64_t n, T alpha, const T* __restrict__ dinv, const T* __restrict__ rhs,
+                                 T* __restrict__ d, T* __restrict__ x, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T z = mul_rn(dinv[i], rhs[i]);
+  d[i] = z;
+  x[i] = mul_rn(alpha, z);
+}
+
+cudaError_t launch_cheb_zero(DType t, int64_t n, double alpha, const void* dinv, const void* rhs,
+                             void* d, void* x, const int* guard, cudaStream_t s) {
+  const int nb = div_up(n, 256);
+  if (t == F64)
+    cheb_zero_kernel<double><<<nb, 256, 0, s>>>(n, alpha, (const double*)dinv, (const double*)rhs,
+                                                (double*)d, (double*)x, guard);
+  else
+    cheb_zero_kernel<float><<<nb, 256, 0, s>>>(n, (float)alpha, (const float*)dinv,
+                                               (const float*)rhs, (float*)d, (float*)x, guard);
+  return cudaGetLastError();
+}
+
+// First damped-Jacobi step from x0 = 0: x = (omega * dinv) * rhs.
+template <typename T>
+__global__ void jac_zero_kernel(int64_t n, T omega, const T* __restrict__ dinv, const T* __restrict__ rhs,
+                                T* __restrict__ x, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = mul_rn(mul_rn(omega, dinv[i]), rhs[i]);
+}
+
+cudaError_t launch_jac_zero(DType t, int64_t n, double omega, const void* dinv, const void* rhs,
+                            void* x, const int* guard, cudaStream_t s) {
+  const int nb = div_up(n, 256);
+  if (t == F64)
+    jac_zero_kernel<double><<<nb, 256, 0, s>>>(n, omega, (const double*)dinv, (const double*)rhs,
+                                               (double*)x, guard);
+  else
+    jac_zero_kernel<float><<<nb, 256, 0, s>>>(n, (float)omega, (const float*)dinv,
+                                              (const float*)rhs, (float*)x, guard);
+  return cudaGetLastError();
+}
+
+template <typename T>
+__global__ void expand_kernel(int64_t nf, const int32_t* __restrict__ idx, const T* __restrict__ src,
+                              T* __restrict__ dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nf) dst[idx[i]] = src[i];
+}
+template <typename T>
+__global__ void compress_kernel(int64_t nf, const int32_t* __restrict__ idx, const T* __restrict__ src,
+                                T* __restrict__ dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nf) dst[i] = src[idx[i]];
+}
+
+cudaError_t launch_expand(DType t, int64_t n_free, const int32_t* free_idx, const void* src_free,
+                          void* dst_full, cudaStream_t s) {
+  const int nb = div_up(n_free, 256);
+  if (t == F64)
+    expand_kernel<double><<<nb, 256, 0, s>>>(n_free, free_idx, (const double*)src_free, (double*)dst_full);
+  else
+    expand_kernel<float><<<nb, 256, 0, s>>>(n_free, free_idx, (const float*)src_free, (float*)dst_full);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compress(DType t, int64_t n_free, const int32_t* free_idx,
+                            const void* src_full, void* dst_free, cudaStream_t s) {
+  const int nb = div_up(n_free, 256);
+  if (t == F64)
+    compress_kernel<double><<<nb, 256, 0, s>>>(n_free, free_idx, (const double*)src_full, (double*)dst_free);
+  else
+    compress_kernel<float><<<nb, 256, 0, s>>>(n_free, free_idx, (const float*)src_full, (float*)dst_free);
+  return cudaGetLastError();
+}
+
+__global__ void gather_idx_kernel(int64_t n, const int32_t* __restrict__ idx, const double* __restrict__ src,
+                                  double* __restrict__ dst, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[idx[i]];
+}
+__global__ void scatter_idx_kernel(int64_t n, const int32_t* __restrict__ idx, const double* __restrict__ src,
+                                   double* __restrict__ dst, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[idx[i]] = src[i];
+}
+
+cudaError_t launch_gather_idx(int64_t n, const int32_t* idx, const double* src, double* dst,
+                              const int* guard, cudaStream_t s) {
+  gather_idx_kernel<<<div_up(n, 256), 256, 0, s>>>(n, idx, src, dst, guard);
+  return cudaGetLastError();
+}
+cudaError_t launch_scatter_idx(int64_t n, const int32_t* idx, const double* src, double* dst,
+                               const int* guard, cudaStream_t s) {
+  scatter_idx_kernel<<<div_up(n, 256), 256, 0, s>>>(n, idx, src, dst, guard);
+  return cudaGetLastError();
+}
+
+// out = mask ? op(a) : 0 with
+//   op 0: 1 / a          op 1: a * s          op 2: a / s (s_dev when given)
+//   op 3: b * a          op 4: s (constant)   op 5: a
+//   op 6: |a| > 1e-12 ? a : 1   (the reference's diagonal guard)
+__global__ void vec_op_kernel(int64_t n, int op, const double* __restrict__ a, const double* __restrict__ b,
+                              const uint8_t* __restrict__ mask, double s, const double* s_dev,
+                              double* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bool m = mask == nullptr || mask[i] != 0;
+  double r = 0.0;
+  if (m) {
+    switch (op) {
+      case 0: r = 1.0 / a[i]; break;
+      case 1: r = a[i] * s; break;
+      case 2: r = a[i] / (s_dev != nullptr ? *s_dev : s); break;
+      case 3: r = b[i] * a[i]; break;
+      case 4: r = s; break;
+      case 5: r = a[i]; break;
+      case 6: r = fabs(a[i]) > 1e-12 ? a[i] : 1.0; break;
+      default: r = a[i];
+    }
+  }
+  out[i] = r;
+}
+
+cudaError_t launch_vec_op(int64_t n, int op, const double* a, const double* b, const uint8_t* mask,
+                          double s, const double* s_dev, double* out, cudaStream_t st) {
+  vec_op_kernel<<<div_up(n, 256), 256, 0, st>>>(n, op, a, b, mask, s, s_dev, out);
+  return cudaGetLastError();
+}
+
+// Root-enrichment weights (gpu_fem/multigrid_v4.py:1150-1157):
+// w = clip(|diag| / max|diag|, floor, 1) ** power on free DOFs.
+__global__ void enrich_weight_kernel(int64_t n, const double* __restrict__ diag, const uint8_t* __restrict__ mask,
+                                     const double* __restrict__ dmax, double wfloor, double wpow,
+                                     double* __restrict__ w) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!mask[i]) {
+    w[i] = 0.0;
+    return;
+  }
+  double v = fabs(diag[i]) / fmax(*dmax, 1e-300);
+  v = fmin(fmax(v, wfloor), 1.0);
+  if (fabs(wpow - 1.0) > 1e-12) v = pow(v, wpow);
+  w[i] = v;
+}
+
+cudaError_t launch_enrich_weights(int64_t n, const double* diag, const uint8_t* mask,
+                                  const double* dmax_dev, double wfloor, double wpow, double* w,
+                                  cudaStream_t s) {
+  enrich_weight_kernel<<<div_up(n, 256), 256, 0, s>>>(n, diag, mask, dmax_dev, wfloor, wpow, w);
+  return cudaGetLastError();
+}
+
+// out = mask ? (mode 0: w * r ; mode 1: clip(1 - w, floor, 1) * r ;
+//               mode 2: w * (r - p) ; mode 3: clip(1 - w, floor, 1) * (r - p)) : 0
+__global__ void enrich_rhs_kernel(int64_t n, int mode, const double* __restrict__ w, double wfloor,
+                                  const double* __restrict__ r, const double* __restrict__ p,
+                                  const uint8_t* __restrict__ mask, double* __restrict__ out,
+                                  const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!mask[i]) {
+    out[i] = 0.0;
+    return;
+  }
+  double ww = w[i];
+  if (mode == 1 || mode == 3) ww = fmin(fmax(1.0 - ww, wfloor), 1.0);
+  const double rr = (mode >= 2) ? sub_rn(r[i], p[i]) : r[i];
+  out[i] = mul_rn(ww, rr);
+}
+
+cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloor, const double* r,
+                              const double* p, const uint8_t* mask, double* out, const int* guard,
+                              cudaStream_t s) {
+  enrich_rhs_kernel<<<div_up(n, 256), 256, 0, s>>>(n, mode, w, wfloor, r, p, mask, out, guard);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Dense FP64 Cholesky (lower, row-major, right-looking, 32-wide panels) for the
+// coarsest level (gpu_fem/multigrid_v4.py:1302-1339 uses cp.linalg.cholesky).
+constexpr int NB = 32;
+
+__global__ void potrf_diag_kernel(double* A, int n, int k0, int* info) {
+  __shared__ double T[NB][NB + 1];
+  const int kb = min(NB, n - k0);
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    T[r][c] = (r < kb && c < kb) ? A[(int64_t)(k0 + r) * n + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  for (int j = 0; j < kb; ++j) {
+    if (threadIdx.x == 0) {
+      const double d = T[j][j];
+      if (!(d > 0.0) || !isfinite(d)) {
+        if (*info == 0) *info = k0 + j + 1;
+        T[j][j] = 1.0;
+      } else {
+        T[j][j] = sqrt(d);
+      }
+    }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) T[i][j] /= T[j][j];
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+      const int i = idx / NB, c = idx % NB;
+      if (i > j && c > j && c <= i && i < kb) T[i][c] -= T[i][j] * T[c][j];
+    }
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    if (r < kb && c < kb) A[(int64_t)(k0 + r) * n + k0 + c] = (c <= r) ? T[r][c] : 0.0;
+  }
+}
+
+// rows i >= k0 + kb: A[i, k0:k0+kb] <- A[i, k0:k0+kb] * L_kk^{-T}
+__global__ void trsm_panel_kernel(double* A, int n, int k0) {
+  __shared__ double L[NB][NB + 1];
+  const int kb = min(NB, n - k0);
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    L[r][c] = (r < kb && c < kb) ? A[(int64_t)(k0 + r) * n + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  const int i = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x[NB];
+  double* row = A + (int64_t)i * n + k0;
+  for (int j = 0; j < kb; ++j) {
+    double a = row[j];
+    for (int p = 0; p < j; ++p) a -= x[p] * L[j][p];
+    x[j] = a / L[j][j];
+  }
+  for (int j = 0; j < kb; ++j) row[j] = x[j];
+}
+
+// trailing update A[i][j] -= sum_p A[i][k0+p] * A[j][k0+p], lower tiles only
+__global__ void syrk_update_kernel(double* A, int n, int k0) {
+  const int kb = min(NB, n - k0);
+  const int start = k0 + kb;
+  const int ti = blockIdx.y, tj = blockIdx.x;
+  if (tj > ti) return;
+  const int i0 = start + ti * NB, j0 = start + tj * NB;
+  __shared__ double Pi[NB][NB + 1], Pj[NB][NB + 1];
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    Pi[r][c] = (i0 + r < n && c < kb) ? A[(int64_t)(i0 + r) * n + k0 + c] : 0.0;
+    Pj[r][c] = (j0 + r < n && c < kb) ? A[(int64_t)(j0 + r) * n + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    const int i = i0 + r, j = j0 + c;
+    if (i >= n || j >= n || j > i) continue;
+    double s = 0.0;
+#pragma unroll 8
+    for (int p = 0; p < NB; ++p) s += Pi[r][p] * Pj[c][p];
+    A[(int64_t)i * n + j] -= s;
+  }
+}
+
+cudaError_t dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s) {
+  cudaMemsetAsync(info_dev, 0, sizeof(int), s);
+  for (int k0 = 0; k0 < n; k0 += NB) {
+    potrf_diag_kernel<<<1, 256, 0, s>>>(A, n, k0, info_dev);
+    const int kb = std::min(NB, n - k0);
+    const int rest = n - k0 - kb;
+    if (rest > 0) {
+      trsm_panel_kernel<<<div_up(rest, 128), 128, 0, s>>>(A, n, k0);
+      const int nt = div_up(rest, NB);
+      syrk_update_kernel<<<dim3(nt, nt), 256, 0, s>>>(A, n, k0);
+    }
+  }
+  // zero the strict upper triangle so the factor is a clean lower matrix
+  return cudaGetLastError();
+}
+
+// Linv = L^{-1}: block of 32 columns per CTA, forward substitution row by row.
+__global__ void tri_inverse_kernel(const double* __restrict__ L, int n, double* __restrict__ Linv) {
+  const int c0 = blockIdx.x * NB;
+  const int cb = min(NB, n - c0);
+  const int col = threadIdx.x & (NB - 1);   // 32 columns
+  const int part = threadIdx.x >> 5;        // 8 partial sums per column
+  const int nparts = blockDim.x >> 5;
+  __shared__ double red[8][NB];
+  // rows < c0 are zero
+  for (int r = c0; r < n; ++r) {
+    double s = 0.0;
+    if (col < cb) {
+      for (int j = c0 + part; j < r; j += nparts) s += L[(int64_t)r * n + j] * Linv[(int64_t)j * n + c0 + col];
+    }
+    red[part][col] = s;
+    __syncthreads();
+    if (part == 0 && col < cb) {
+      double t = 0.0;
+      for (int p = 0; p < nparts; ++p) t += red[p][col];
+      const double e = (r == c0 + col) ? 1.0 : 0.0;
+      Linv[(int64_t)r * n + c0 + col] = (r < c0 + col) ? 0.0 : (e - t) / L[(int64_t)r * n + r];
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t dense_inverse_from_chol(const double* L, int n, double* Linv, double* /*work*/,
+                                    cudaStream_t s) {
+  cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, s);
+  tri_inverse_kernel<<<div_up(n, NB), 256, 0, s>>>(L, n, Linv);
+  return cudaGetLastError();
+}
+
+// t = Linv b (warp per row) ; x = Linv^T t (thread per column)
+__global__ void trmv_lower_kernel(const double* __restrict__ Li, int n, const double* __restrict__ b,
+                                  double* __restrict__ t, const int* guard) {
+  if (guard_off(guard)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  double s = 0.0;
+  const double* row = Li + (int64_t)warp * n;
+  for (int j = lane; j <= warp; j += 32) s += row[j] * b[j];
+  s = warp_sum(s);
+  if (lane == 0) t[warp] = s;
+}
+
+__global__ void trmv_lowerT_kernel(const double* __restrict__ Li, int n, const double* __restrict__ t,
+                                   double* __restrict__ x, const int* guard) {
+  if (guard_off(guard)) return;
+  // block of 32 columns x 8 row-slices, reduced in shared memory
+  const int col = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int part = threadIdx.x >> 5;
+  __shared__ double red[8][32];
+  double s = 0.0;
+  if (col < n)
+    for (int i = col + part; i < n; i += 8) s += Li[(int64_t)i * n + col] * t[i];
+  red[part][threadIdx.x & 31] = s;
+  __syncthreads();
+  if (part == 0 && col < n) {
+    double a = 0.0;
+    for (int p = 0; p < 8; ++p) a += red[p][threadIdx.x & 31];
+    x[col] = a;
+  }
+}
+
+cudaError_t launch_coarsest_solve(const double* Linv, int n, const double* b, double* tmp,
+                                  double* x, const int* guard, cudaStream_t s) {
+  trmv_lower_kernel<<<div_up((int64_t)n * 32, 256), 256, 0, s>>>(Linv, n, b, tmp, guard);
+  trmv_lowerT_kernel<<<div_up(n, 32), 256, 0, s>>>(Linv, n, tmp, x, guard);
+  return cudaGetLastError();
+}
+
+__global__ void add_diag_kernel(double* A, int n, double eps) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[(int64_t)i * n + i] += eps;
+}
+cudaError_t launch_add_diag(double* A, int n, double eps, cudaStream_t s) {
+  add_diag_kernel<<<div_up(n, 256), 256, 0, s>>>(A, n, eps);
+  return cudaGetLastError();
+}
+
+__global__ void diag_sum_kernel(const double* A, int n, double* out) {
+  // single block
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += A[(int64_t)i * n + i];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    *out = t;
+  }
+}
+cudaError_t launch_diag_sum(const double* A, int n, double* out, cudaStream_t s) {
+  diag_sum_kernel<<<1, 256, 0, s>>>(A, n, out);
+  return cudaGetLastError();
+}
+
+__global__ void all_finite_kernel(const double* A, int64_t n, int* flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !isfinite(A[i])) *flag = 1;
+}
+cudaError_t launch_all_finite(const double* A, int64_t n, int* flag, cudaStream_t s) {
+  all_finite_kernel<<<div_up(n, 256), 256, 0, s>>>(A, n, flag);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Krylov building blocks (_cupy_fgmres, gpu_fem/multigrid_v4.py:416-534), the
+// Arnoldi state living on the device.
+
+// h[0] = <v0, w>
+cudaError_t launch_mgs_first(int64_t n, const double* v0, const double* w, RedWork rw, double* h0,
+                             const int* guard, cudaStream_t s) {
+  DotSet ds;
+  ds.a[0] = v0;
+  ds.b[0] = w;
+  ds.nd = 1;
+  return launch_dots(F64, n, ds, rw, h0, guard, s);
+}
+
+// w <- w - h_i * v_i ; out <- <v_next, w_new> (or <w_new, w_new> when v_next is null)
+__global__ void __launch_bounds__(kRedThreads) mgs_step_kernel(int64_t n, const double* __restrict__ vi,
+                                                               const double* __restrict__ vnext,
+                                                               double* __restrict__ w,
+                                                               const double* __restrict__ hi, RedWork rw,
+                                                               double* out, const int* guard) {
+  if (guard_off(guard)) return;
+  __shared__ double sh[32];
+  const double h = *hi;
+  double v[1] = {0.0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double wn = sub_rn(w[i], mul_rn(h, vi[i]));
+    w[i] = wn;
+    v[0] += (vnext != nullptr ? vnext[i] : wn) * wn;
+  }
+  block_sum<1>(v, sh);
+  last_block_finalize<1>(v, rw, out);
+}
+
+cudaError_t launch_mgs_step(int64_t n, const double* vi, const double* vnext, double* w,
+                            const double* hi, RedWork rw, double* out, const int* guard,
+                            cudaStream_t s) {
+  mgs_step_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(n, vi, vnext, w, hi, rw, out, guard);
+  return cudaGetLastError();
+}
+
+// Krylov control (single thread).  Flags: see KrylovDev in internal.h.
+__global__ void krylov_init_kernel(KrylovDev k, const int* parent) {
+  int* f = k.flags;
+  const bool pok = parent == nullptr || *parent != 0;
+  const double bn = sqrt(k.sc[SC_BNORM2]);
+  k.sc[SC_BNORM] = bn;
+  for (int i = 0; i < NFLAGS; ++i) f[i] = 0;
+  f[F_HISTN] = 0;
+  if (!pok) {
+    f[F_DONE] = 1;
+  } else if (bn <= 1e-30) {
+    f[F_DONE] = 1;
+    f[F_CONV] = 1;
+  }
+  f[F_NOTDONE] = f[F_DONE] ? 0 : 1;
+}
+
+__global__ void krylov_restart_kernel(KrylovDev k, double tol, double* hist_host, int hist_cap) {
+  int* f = k.flags;
+  f[F_DID] = 0;
+  f[F_CYC] = 0;
+  if (f[F_DONE]) return;
+  const double beta = sqrt(k.sc[SC_BETA2]);
+  k.sc[SC_BETA] = beta;
+  const double rel = beta / k.sc[SC_BNORM];
+  if (hist_host != nullptr && f[F_HISTN] < hist_cap) hist_host[f[F_HISTN]] = rel;
+  f[F_HISTN] += 1;
+  if (rel <= tol) {
+    f[F_DONE] = 1;
+    f[F_CONV] = 1;
+    f[F_NOTDONE] = 0;
+    return;
+  }
+  f[F_CYC] = 1;
+  f[F_DID] = 1;
+  f[F_JF] = 0;
+  k.g[0] = beta;
+}
+
+// Givens update of column j (the reference's host-side loop, done on the device).
+__global__ void givens_kernel(KrylovDev k, int j, double tol, double* hist_host, int hist_cap) {
+  int* f = k.flags;
+  if (!f[F_CYC]) return;
+  const int ld = k.restart + 1;
+  double* H = k.H + (int64_t)j * ld;  // column j
+  const double h_norm = sqrt(k.sc[SC_HSQ]);
+  H[j + 1] = h_norm;
+  k.sc[SC_HNORM] = h_norm;
+  for (int i = 0; i < j; ++i) {
+    const double a = H[i], b = H[i + 1];
+    const double tmp = __dadd_rn(__dmul_rn(k.cs[i], a), __dmul_rn(k.sn[i], b));
+    H[i + 1] = __dadd_rn(__dmul_rn(-k.sn[i], a), __dmul_rn(k.cs[i], b));
+    H[i] = tmp;
+  }
+  const double hjj = H[j], hj1 = H[j + 1];
+  const double denom = sqrt(__dadd_rn(__dmul_rn(hjj, hjj), __dmul_rn(hj1, hj1)));
+  double c, sn;
+  if (denom < 1e-300) {
+    c = 1.0;
+    sn = 0.0;
+  } else {
+    c = hjj / denom;
+    sn = hj1 / denom;
+  }
+  k.cs[j] = c;
+  k.sn[j] = sn;
+  H[j] = __dadd_rn(__dmul_rn(c, hjj), __dmul_rn(sn, hj1));
+  H[j + 1] = 0.0;
+  const double gj = k.g[j];
+  k.g[j + 1] = __dmul_rn(-sn, gj);
+  k.g[j] = __dmul_rn(c, gj);
+  f[F_TOTAL] += 1;
+  f[F_JF] = j + 1;
+  const double rel = fabs(k.g[j + 1]) / k.sc[SC_BNORM];
+  if (hist_host != nullptr && f[F_HISTN] < hist_cap) hist_host[f[F_HISTN]] = rel;
+  f[F_HISTN] += 1;
+  if (rel <= tol) {
+    f[F_CONV] = 1;
+    f[F_DONE] = 1;
+    f[F_NOTDONE] = 0;
+    f[F_CYC] = 0;
+  } else if (h_norm <= 1e-14) {
+    // lucky breakdown: the reference reports convergence
+    f[F_CONV] = 1;
+    f[F_DONE] = 1;
+    f[F_NOTDONE] = 0;
+    f[F_BREAK] = 1;
+    f[F_CYC] = 0;
+  }
+}
+
+// dst = src / (*denom)   (V[j+1] = w / h_norm ; V[0] = r / beta)
+__global__ void scale_vec_kernel(int64_t n, const double* __restrict__ src, const double* __restrict__ denom,
+                                 double* __restrict__ dst, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i] / *denom;
+}
+
+cudaError_t launch_scale_vec(int64_t n, const double* src, const double* denom_dev, double* dst,
+                             const int* guard, cudaStream_t s) {
+  scale_vec_kernel<<<div_up(n, 256), 256, 0, s>>>(n, src, denom_dev, dst, guard);
+  return cudaGetLastError();
+}
+
+// Back substitution R y = g[:jf] (column-oriented, R = triu(H[:jf, :jf])).
+// A zero pivot (exactly singular R; the reference falls back to lstsq) sets y_j = 0.
+__global__ void backsolve_kernel(KrylovDev k) {
+  if (!k.flags[F_DID]) return;
+  const int jf = k.flags[F_JF];
+  const int ld = k.restart + 1;
+  __shared__ double x[1024];
+  for (int i = threadIdx.x; i < jf; i += blockDim.x) x[i] = k.g[i];
+  __syncthreads();
+  for (int j = jf - 1; j >= 0; --j) {
+    if (threadIdx.x == 0) {
+      const double r = k.H[(int64_t)j * ld + j];
+      x[j] = (r != 0.0) ? x[j] / r : 0.0;
+    }
+    __syncthreads();
+    const double xj = x[j];
+    for (int i = threadIdx.x; i < j; i += blockDim.x) x[i] = __dsub_rn(x[i], __dmul_rn(xj, k.H[(int64_t)j * ld + i]));
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < jf; i += blockDim.x) k.y[i] = x[i];
+}
+
+cudaError_t launch_backsolve(KrylovDev k, cudaStream_t s) {
+  backsolve_kernel<<<1, 256, 0, s>>>(k);
+  return cudaGetLastError();
+}
+
+// x <- x + y_0 Z_0 + y_1 Z_1 + ... (sequential per element, as the reference's loop)
+__global__ void update_x_kernel(int64_t n, double* __restrict__ x, double* const* __restrict__ Z,
+                                const double* __restrict__ y, const int* flags) {
+  if (!flags[F_DID]) return;
+  const int jf = flags[F_JF];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double xi = x[i];
+  for (int j = 0; j < jf; ++j) xi = __dadd_rn(xi, __dmul_rn(y[j], Z[j][i]));
+  x[i] = xi;
+}
+
+cudaError_t launch_update_x(int64_t n, double* x, double* const* Z_dev, const double* y,
+                            const int* flags, cudaStream_t s) {
+  update_x_kernel<<<div_up(n, 256), 256, 0, s>>>(n, x, Z_dev, y, flags);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Scalar decisions of the safeguarded corrections (single thread).
+//  OP_LS1: coarse-correction line search, first half
+//          (gpu_fem/multigrid_v4.py:867-931): in  sc[0]=|c|^2 sc[1]=|r|^2
+//          sc[2]=<Ac,Ac> sc[3]=<r,Ac> ; out sc[4]=applied scale, sc[7]=degenerate
+//  OP_LS2: second half: in sc[5]=|trial|^2 ; p0 = acceptance ratio ; out sc[6]=accept
+//  OP_RLF: root-local inner FGMRES acceptance (:964-1004): in sc[0]=|c|^2 sc[1]=|r|^2
+//          sc[5]=|trial|^2 ; out sc[6]=accept (scale 1 in sc[4])
+//  OP_RLL: root-local line search (:1006-1055): in sc[0..3] ; p1 = max scale ;
+//          out sc[4]=scale, sc[6]=accept
+__global__ void scalar_op_kernel(int op, double* sc, double p0, double p1, const int* guard) {
+  if (guard_off(guard)) return;
+  if (op == OP_LS1 || op == OP_RLL) {
+    const double cn = sqrt(sc[0]), rn = sqrt(sc[1]);
+    double deg = (cn <= 1e-300 || rn <= 1e-300) ? 1.0 : 0.0;
+    const double denom = sc[2];
+    if (denom <= 1e-300) deg = 1.0;
+    const double raw = sc[3] / denom;
+    const double applied = fmin(p1, fmax(0.0, raw));
+    sc[4] = deg != 0.0 ? 0.0 : applied;
+    sc[7] = deg;
+    sc[8] = raw;
+    if (op == OP_RLL) sc[6] = (deg == 0.0 && applied > 1e-12) ? 1.0 : 0.0;
+  } else if (op == OP_LS2) {
+    const double rn = sqrt(sc[1]);
+    const double tn = sqrt(sc[5]);
+    const bool reject = sc[7] != 0.0 || tn > p0 * rn;
+    sc[6] = reject ? 0.0 : 1.0;
+  } else if (op == OP_RLF) {
+    const double cn = sqrt(sc[0]), rn = sqrt(sc[1]);
+    const bool deg = cn <= 1e-300 || rn <= 1e-300;
+    const double tn = sqrt(sc[5]);
+    sc[4] = 1.0;
+    sc[6] = (!deg && !(tn > rn)) ? 1.0 : 0.0;
+  }
+}
+
+cudaError_t launch_scalar_op(int op, double* sc, double p0, double p1, const int* guard,
+                             cudaStream_t s) {
+  scalar_op_kernel<<<1, 1, 0, s>>>(op, sc, p0, p1, guard);
+  return cudaGetLastError();
+}
+
+// x <- accept ? x + s * c : x   (s = 1 uses x + c)
+template <typename T>
+__global__ void select_axpy_kernel(int64_t n, T* __restrict__ x, const T* __restrict__ c,
+                                   const double* __restrict__ sc, int unit, const int* guard) {
+  if (guard_off(guard)) return;
+  if (sc[6] == 0.0) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T s = (T)sc[4];
+  x[i] = unit ? add_rn(x[i], c[i]) : add_rn(x[i], mul_rn(s, c[i]));
+}
+
+cudaError_t launch_select_axpy(DType t, int64_t n, void* x, const void* c, const double* sc,
+                               int unit, const int* guard, cudaStream_t s) {
+  if (t == F64)
+    select_axpy_kernel<double><<<div_up(n, 256), 256, 0, s>>>(n, (double*)x, (const double*)c, sc,
+                                                              unit, guard);
+  else
+    select_axpy_kernel<float><<<div_up(n, 256), 256, 0, s>>>(n, (float*)x, (const float*)c, sc,
+                                                             unit, guard);
+  return cudaGetLastError();
+}
+
+// trial = r - s * Ac (s from sc[4], or 1 when unit) ; sc[5] = |trial|^2
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) trial_kernel(int64_t n, const T* __restrict__ r,
+                                                            const T* __restrict__ Ac, double* sc,
+                                                            int unit, T* __restrict__ trial,
+                                                            RedWork rw, const int* guard) {
+  if (guard_off(guard)) return;
+  __shared__ double sh[32];
+  const T s = (T)sc[4];
+  double v[1] = {0.0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const T t = unit ? sub_rn(r[i], Ac[i]) : sub_rn(r[i], mul_rn(s, Ac[i]));
+    if (trial != nullptr) trial[i] = t;
+    v[0] += (double)t * (double)t;
+  }
+  block_sum<1>(v, sh);
+  last_block_finalize<1>(v, rw, sc + 5);
+}
+
+cudaError_t launch_trial_residual(DType t, int64_t n, const void* r, const void* Ac, double* sc,
+                                  int unit, void* trial, RedWork rw, const int* guard,
+                                  cudaStream_t s) {
+  if (t == F64)
+    trial_kernel<double><<<red_blocks(n), kRedThreads, 0, s>>>(n, (const double*)r, (const double*)Ac,
+                                                               sc, unit, (double*)trial, rw, guard);
+  else
+    trial_kernel<float><<<red_blocks(n), kRedThreads, 0, s>>>(n, (const float*)r, (const float*)Ac, sc,
+                                                              unit, (float*)trial, rw, guard);
+  return cudaGetLastError();
+}
+
+// Select between the accepted trial residual and the old residual:
+// out <- accept ? trial : r  (used when a corrected residual feeds a second correction)
+template <typename T>
+__global__ void select_vec_kernel(int64_t n, const T* trial, const T* r, const double* sc, T* out,
+                                  const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = sc[6] != 0.0 ? trial[i] : r[i];
+}
+
+cudaError_t launch_select_vec(DType t, int64_t n, const void* trial, const void* r,
+                              const double* sc, void* out, const int* guard, cudaStream_t s) {
+  if (t == F64)
+    select_vec_kernel<double><<<div_up(n, 256), 256, 0, s>>>(n, (const double*)trial, (const double*)r,
+                                                             sc, (double*)out, guard);
+  else
+    select_vec_kernel<float><<<div_up(n, 256), 256, 0, s>>>(n, (const float*)trial, (const float*)r,
+                                                            sc, (float*)out, guard);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_krylov_init(KrylovDev k, const int* parent, cudaStream_t s) {
+  krylov_init_kernel<<<1, 1, 0, s>>>(k, parent);
+  return cudaGetLastError();
+}
+cudaError_t launch_krylov_restart(KrylovDev k, double tol, double* hist_host, int hist_cap,
+                                  cudaStream_t s) {
+  krylov_restart_kernel<<<1, 1, 0, s>>>(k, tol, hist_host, hist_cap);
+  return cudaGetLastError();
+}
+cudaError_t launch_givens(KrylovDev k, int j, double tol, double* hist_host, int hist_cap,
+                          cudaStream_t s) {
+  givens_kernel<<<1, 1, 0, s>>>(k, j, tol, hist_host, hist_cap);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Fixed-count Jacobi-PCG coarse solve (gpu_fem/solver_v2.py:781-810).
+// sc: [0]=rz [1]=pAp [2]=rz_new [3]=alpha [4]=beta
+__global__ void pcg_scalar_kernel(int which, double* sc, const int* guard) {
+  if (guard_off(guard)) return;
+  if (which == 0) {
+    sc[3] = sc[0] / (sc[1] + 1e-300);
+  } else {
+    sc[4] = sc[2] / (sc[0] + 1e-300);
+    sc[0] = sc[2];
+  }
+}
+
+cudaError_t launch_pcg_scalar(int which, double* sc, const int* guard, cudaStream_t s) {
+  pcg_scalar_kernel<<<1, 1, 0, s>>>(which, sc, guard);
+  return cudaGetLastError();
+}
+
+// x += alpha p ; r -= alpha Ap ; z = dinv r ; sc[2] = <r, z>
+__global__ void __launch_bounds__(kRedThreads) pcg_xr_kernel(int64_t n, double* __restrict__ x,
+                                                             double* __restrict__ r, double* __restrict__ z,
+                                                             const double* __restrict__ p,
+                                                             const double* __restrict__ Ap,
+                                                             const double* __restrict__ dinv, double* sc,
+                                                             RedWork rw, const int* guard) {
+  if (guard_off(guard)) return;
+  __shared__ double sh[32];
+  const double alpha = sc[3];
+  double v[1] = {0.0};
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    x[i] = __dadd_rn(x[i], __dmul_rn(alpha, p[i]));
+    const double rn = __dsub_rn(r[i], __dmul_rn(alpha, Ap[i]));
+    r[i] = rn;
+    const double zn = __dmul_rn(dinv[i], rn);
+    z[i] = zn;
+    v[0] += rn * zn;
+  }
+  block_sum<1>(v, sh);
+  last_block_finalize<1>(v, rw, sc + 2);
+}
+
+cudaError_t launch_pcg_xr(int64_t n, double* x, double* r, double* z, const double* p, const double* Ap,
+                          const double* dinv, double* sc, RedWork rw, const int* guard, cudaStream_t s) {
+  pcg_xr_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(n, x, r, z, p, Ap, dinv, sc, rw, guard);
+  return cudaGetLastError();
+}
+
+// p = z + beta p
+__global__ void pcg_p_kernel(int64_t n, const double* __restrict__ z, double* __restrict__ p,
+                             const double* __restrict__ sc, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = __dadd_rn(z[i], __dmul_rn(sc[4], p[i]));
+}
+
+cudaError_t launch_pcg_p(int64_t n, const double* z, double* p, const double* sc, const int* guard,
+                         cudaStream_t s) {
+  pcg_p_kernel<<<div_up(n, 256), 256, 0, s>>>(n, z, p, sc, guard);
+  return cudaGetLastError();
+}
+
+// z = dinv * r (elementwise), guarded
+__global__ void dmul_kernel(int64_t n, const double* __restrict__ dinv, const double* __restrict__ r,
+                            double* __restrict__ z, const int* guard) {
+  if (guard_off(guard)) return;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = __dmul_rn(dinv[i], r[i]);
+}
+
+cudaError_t launch_dmul(int64_t n, const double* dinv, const double* r, double* z, const int* guard,
+                        cudaStream_t s) {
+  dmul_kernel<<<div_up(n, 256), 256, 0, s>>>(n, dinv, r, z, guard);
+  return cudaGetLastError();
+}
+
+}  // namespace simpfem

@@ -1,0 +1,180 @@
+"""The guarded SIMP-floor policy: probe -> preserve/escalate -> floor ladder ->
+recomputed true-residual guard.
+
+Follows experiments/phase5/run_gmg_floor_detector_prospective.py:
+``_classify`` (:77-90), ``solve_at_floor`` (:220-261), the r50 / r100 probe
+read-out (:263-277), the optional severity jump (:278-290), the floor sequence
+(:313-349) and the post-solve fallback after a failed keep (:351-354).  The
+density-field variant (run_gmg_floor_detector_density_field.py:180-299) is the
+same policy with E = rho_min + (1 - rho_min) * density ** penal; the Bernoulli
+variant first maps a solid mask to rho = 1 (solid) / rho_min (void).
+
+Every accepted answer passes the FP64 guard ||F - K(E) x|| / ||F|| <= tol,
+recomputed from x after the solve.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .multigrid_v4 import _cupy_fgmres
+from .paper4 import CANONICAL_STACK, _build_components
+
+
+def _classify(r50: float, r100: float, *, high_residual_threshold: float, plateau_residual_threshold: float,
+              plateau_ratio_threshold: float) -> tuple[bool, str]:
+    if r50 >= high_residual_threshold:
+        return True, "high_r50"
+    ratio = r100 / max(r50, 1e-300)
+    if r100 >= plateau_residual_threshold and ratio >= plateau_ratio_threshold:
+        return True, "plateau"
+    return False, "keep"
+
+
+@dataclass
+class FloorAttempt:
+    rho_min: float
+    iters: int
+    solver_reported_converged: bool
+    true_converged: bool
+    final_rel_residual: float
+    setup_time_s: float
+    solve_time_s: float
+    history: list = field(default_factory=list)
+
+
+class GuardedFloorPolicy:
+    """One hierarchy reused across states (as the drivers do), so the lambda_max
+    cache carries over from state to state exactly like the reference."""
+
+    def __init__(self, preset="cantilever_gpu_medium", *, penal: float = 4.5, tol: float = 1e-6,
+                 restart: int = 300, maxiter: int = 300, probe_iters: int = 100, probe_r50: int = 50,
+                 baseline_rho_min: float = 1e-12, raised_rho_mins: Sequence[float] = (1e-3,),
+                 high_residual_threshold: float = 1e-2, plateau_residual_threshold: float = 1e-4,
+                 plateau_ratio_threshold: float = 0.6, severity_jump_r50_threshold: float = 0.0,
+                 severity_jump_rho_min: float = 1e-2, stack: Optional[dict] = None, n_levels: int = 4,
+                 cycle_precision: str = "fp64"):
+        flags = dict(CANONICAL_STACK if stack is None else stack)
+        (self.spec, self.bc, self.free, self.free_gpu, self.edof_gpu, self.F_free_gpu, self.mf_op,
+         self.gmg) = _build_components(preset, n_levels=n_levels, cycle_precision=cycle_precision, **flags)
+        torch = _lib.require_cuda()
+        self.penal = float(penal)
+        self.tol = float(tol)
+        self.restart = int(restart)
+        self.maxiter = int(maxiter)
+        self.probe_iters = int(probe_iters)
+        self.probe_r50 = int(probe_r50)
+        self.baseline_rho_min = float(baseline_rho_min)
+        self.raised_rho_mins = [float(v) for v in raised_rho_mins]
+        self.thresholds = dict(high_residual_threshold=high_residual_threshold,
+                               plateau_residual_threshold=plateau_residual_threshold,
+                               plateau_ratio_threshold=plateau_ratio_threshold)
+        self.severity_jump_r50_threshold = float(severity_jump_r50_threshold)
+        self.severity_jump_rho_min = float(severity_jump_rho_min)
+        self.b_norm = float(torch.linalg.norm(self.F_free_gpu))
+        self.last_x = None
+
+    # ---------------------------------------------------------------- moduli
+    def moduli(self, density, rho_min: float, *, binary: bool = False):
+        """E = rho_min + (1 - rho_min) * rho ** penal on the device.  ``binary``:
+        ``density`` is a solid mask and void elements take rho = rho_min."""
+        torch = _lib.require_cuda()
+        d = _lib.as_cuda(density, torch.float64)
+        if binary:
+            rho = torch.where(d != 0, torch.ones_like(d), torch.full_like(d, rho_min))
+        else:
+            rho = d
+        return rho_min + (1.0 - rho_min) * rho ** self.penal
+
+    def solve_at_floor(self, density, rho_min: float, *, maxiter: int, history: list, binary: bool = False,
+                       x0=None) -> FloorAttempt:
+        torch = _lib.require_cuda()
+        E_e = self.moduli(density, rho_min, binary=binary)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        self.gmg.setup(E_e)
+        torch.cuda.synchronize()
+        setup_time = time.perf_counter() - t0
+
+        def A_op(x):
+            return self.mf_op.matvec(x, E_e)
+
+        t0 = time.perf_counter()
+        x, iters, reported = _cupy_fgmres(A_op, self.F_free_gpu, self.gmg.apply, x0=x0, tol=self.tol,
+                                          maxiter=maxiter, restart=self.restart, history=history)
+        torch.cuda.synchronize()
+        solve_time = time.perf_counter() - t0
+        final = float(torch.linalg.norm(self.F_free_gpu - A_op(x)) / self.b_norm)
+        self.last_x = x
+        return FloorAttempt(rho_min, int(iters), bool(reported), final <= self.tol, final, setup_time, solve_time,
+                            list(history))
+
+    # ---------------------------------------------------------------- policy
+    def run(self, density, *, binary: bool = False) -> dict:
+        probe_history: list = []
+        probe = self.solve_at_floor(density, self.baseline_rho_min, maxiter=self.probe_iters,
+                                    history=probe_history, binary=binary)
+        r50 = probe_history[min(self.probe_r50, len(probe_history) - 1)]
+        r100 = probe_history[min(self.probe_iters, len(probe_history) - 1)]
+        raise_floor, trigger = _classify(r50, r100, **self.thresholds)
+        severity = raise_floor and self.severity_jump_r50_threshold > 0.0 and r50 >= self.severity_jump_r50_threshold
+        if raise_floor and severity:
+            ladder = [v for v in self.raised_rho_mins if v >= self.severity_jump_rho_min] or [self.severity_jump_rho_min]
+        else:
+            ladder = self.raised_rho_mins if raise_floor else [self.baseline_rho_min]
+        attempts: list[FloorAttempt] = []
+        attempted: list[float] = []
+        state = {"selected": None}
+
+        def run_sequence(seq):
+            for rho_min in seq:
+                if rho_min in attempted:
+                    continue
+                attempted.append(rho_min)
+                a = self.solve_at_floor(density, rho_min, maxiter=self.maxiter, history=[], binary=binary)
+                attempts.append(a)
+                state["selected"] = a
+                if a.true_converged:
+                    break
+
+        run_sequence(ladder)
+        sel = state["selected"]
+        fallback = False
+        if (sel is None or not sel.true_converged) and not raise_floor:
+            fallback = True
+            run_sequence(self.raised_rho_mins)
+            sel = state["selected"]
+        failed = [a for a in attempts if a is not sel]
+        return {
+            "probe_r50": r50,
+            "probe_r100": r100,
+            "probe_r100_over_r50": r100 / max(r50, 1e-300),
+            "probe_setup_time_s": probe.setup_time_s,
+            "probe_solve_time_s": probe.solve_time_s,
+            "probe_iters": probe.iters,
+            "trigger": trigger,
+            "predicted_raise_floor": int(raise_floor),
+            "severity_jump_triggered": int(severity),
+            "post_solve_fallback_triggered": int(fallback),
+            "detector_false_keep": int((not raise_floor) and fallback),
+            "recommended_rho_min": sel.rho_min if sel else (ladder[-1] if ladder else float("nan")),
+            "attempted_rho_mins": ";".join(f"{v:.0e}" for v in attempted),
+            "n_floor_attempts": len(attempted),
+            "solve_converged": int(bool(sel and sel.true_converged)),
+            "solver_reported_converged": int(bool(sel and sel.solver_reported_converged)),
+            "solve_iters": sel.iters if sel else self.maxiter,
+            "solve_final_rel_residual": sel.final_rel_residual if sel else float("nan"),
+            "selected_setup_time_s": sel.setup_time_s if sel else float("nan"),
+            "selected_solve_time_s": sel.solve_time_s if sel else float("nan"),
+            "failed_ladder_setup_time_s": sum(a.setup_time_s for a in failed),
+            "failed_ladder_solve_time_s": sum(a.solve_time_s for a in failed),
+            "recorded_policy_time_s": probe.setup_time_s + probe.solve_time_s
+            + sum(a.setup_time_s + a.solve_time_s for a in attempts),
+            "probe_history": probe_history,
+            "attempts": attempts,
+        }

@@ -1,0 +1,286 @@
+"""Generate the golden fixtures in this folder from the reference itself.
+
+Run from the repository root on a machine where the reference source tree is
+readable (default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+
+    python tests/golden/make_golden.py
+
+Every number written here comes from the reference's own unmodified Python
+(``gpu_fem.solver_v2.MatrixFreeKff``, ``gpu_fem.multigrid_v4.GalerkinMatFreeGMG``,
+``_cupy_fgmres``, ``_cupy_pcg``, ``NodeBlockJacobiMF``, ``generate_bc`` and the
+phase-5 prospective driver), executed on the host through the numpy-backed
+``cupy`` stand-in in ``_refshim.py``.  The fixtures pin the oracle restatement
+under ``oracle/`` and, through it, the CUDA path.
+
+Published per-state values (``published_*.csv``) and the two stored density
+fields are extracted verbatim from the reference's deposited data tables.
+"""
+
+from __future__ import annotations
+
+import csv
+import os
+import shutil
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import _refshim  # noqa: E402
+
+# Stacks exercised against the reference (keyword arguments of
+# GalerkinMatFreeGMG, multigrid_v4.py:546-580).
+STACKS = {
+    "plain_jacobi": dict(smoother_type="jacobi"),
+    "plain_cheb": dict(),
+    "line_search": dict(coarse_correction_policy="residual_line_search"),
+    "canonical": dict(
+        coarse_correction_policy="residual_line_search",
+        root_local_correction_mode="node_block_inner_fgmres",
+        root_local_correction_inner_steps=20,
+        root_local_correction_inner_restart=20,
+        inner_krylov_steps=10,
+        inner_krylov_restart=10,
+    ),
+    "wcycle": dict(cycle_type="w"),
+    "nb_line_search": dict(root_local_correction_mode="node_block_line_search"),
+    "enrich": dict(
+        coarse_correction_policy="residual_line_search",
+        root_enrichment_mode="weighted_gap_second",
+    ),
+    "enrich_void": dict(root_enrichment_mode="void_residual_second"),
+    "level_fp32": dict(level_precisions=["fp64", "fp32", "fp32"]),
+    "fine_fp32": dict(fine_smoother="fp32"),
+}
+
+
+def _cases():
+    ps = _refshim.load("problem_spec")
+    presets = _refshim.load("presets")
+    odd = ps.ProblemSpec(
+        Lx=2.0, Ly=1.0, Lz=0.5, nelx=13, nely=7, nelz=5, volfrac=0.3,
+        supports=[ps.EdgeSupport(edge="left", constraint="fixed")],
+        loads=[ps.PointLoad(x=2.0, y=0.5, z=0.25, fy=-1.0)],
+    )
+    return {
+        "cant24": (presets.get_preset("cantilever_3d"), 3),
+        "odd13": (odd, 3),
+        "bridge30": (presets.get_preset("bridge_3d"), 3),
+    }
+
+
+def _fields(n_elem: int, seed: int):
+    rng = np.random.default_rng(seed)
+    solid = rng.random(n_elem) < 0.35
+    rho_bin = solid.astype(np.float64)
+    smooth = 0.3 + 0.7 * rng.random(n_elem)
+    out = {}
+    for tag, rho, floor, penal in (
+        ("hi", rho_bin, 1e-12, 4.5),
+        ("mid", rho_bin, 1e-2, 4.5),
+        ("lo", smooth, 1e-3, 3.0),
+    ):
+        out[tag] = floor + (1.0 - floor) * rho**penal
+    return out
+
+
+def _build(spec, n_levels, stack):
+    bcg = _refshim.load("bc_generator")
+    sv2 = _refshim.load("solver_v2")
+    mg = _refshim.load("multigrid_v4")
+    pss = _refshim.load("pub_simp_solver")
+    bc = bcg.generate_bc(spec)
+    free = bc.free_dofs.astype(np.int32)
+    edof = pss._edof_table_3d(spec.nelx, spec.nely, spec.nelz).astype(np.int32)
+    mf = sv2.MatrixFreeKff(edof, pss.KE_UNIT_3D, free, len(free), bc.ndof)
+    kwargs = dict(fine_smoother="fp64")
+    kwargs.update(stack)
+    gmg = mg.GalerkinMatFreeGMG(
+        mf_op=mf, free=free, free_gpu=free, nelx=spec.nelx, nely=spec.nely, nelz=spec.nelz,
+        KE_UNIT=pss.KE_UNIT_3D, n_levels=n_levels, **kwargs,
+    )
+    return bc, free, edof, mf, gmg
+
+
+def _coo(K):
+    K = K.tocoo()
+    return np.stack([K.row.astype(np.int64), K.col.astype(np.int64)]), K.data.copy()
+
+
+def make_structural(out):
+    pss = _refshim.load("pub_simp_solver")
+    sv2 = _refshim.load("solver_v2")
+    mg = _refshim.load("multigrid_v4")
+    out["KE_UNIT_3D"] = pss.KE_UNIT_3D
+    out["edof_3x2x2"] = pss._edof_table_3d(3, 2, 2)
+    for (nf, nc) in (((6, 4, 4), (3, 2, 2)), ((7, 5, 3), (3, 2, 1)), ((1, 3, 2), (1, 1, 1))):
+        P = sv2._build_scalar_prolongation(*nf, *nc).toarray()
+        out["Pscalar_%d%d%d" % nf] = P
+    for s in range(2):
+        for t in range(2):
+            for u in range(2):
+                out[f"Ploc_{s}{t}{u}"] = mg._local_prolongation_scalar(s, t, u)
+    H = pss._build_density_filter(6, 4, 1.5, 3)
+    out["filter_643_r15"] = H.toarray()
+
+
+def make_case(name, spec, n_levels, out):
+    mg = _refshim.load("multigrid_v4")
+    sv2 = _refshim.load("solver_v2")
+    bc, free, edof, mf, gmg = _build(spec, n_levels, STACKS["plain_cheb"])
+    n_elem = spec.nelx * spec.nely * spec.nelz
+    pre = f"{name}/"
+    out[pre + "dims"] = np.array([spec.nelx, spec.nely, spec.nelz, n_levels])
+    out[pre + "free"] = free
+    out[pre + "F"] = bc.F
+    fields = _fields(n_elem, 7)
+    rng = np.random.default_rng(11)
+    u = rng.standard_normal(len(free))
+    out[pre + "u"] = u
+    for tag, E in fields.items():
+        out[pre + f"E_{tag}"] = E
+        out[pre + f"Ku_{tag}"] = mf.matvec(u, E)
+        out[pre + f"Ku32_{tag}"] = mf.matvec(u.astype(np.float32), E.astype(np.float32))
+        out[pre + f"diag_{tag}"] = mf.extract_diagonal(E)
+    for lv in range(n_levels):
+        out[pre + f"free_l{lv}"] = gmg._free_per_level[lv]
+    for lv in range(n_levels - 1):
+        ij, v = _coo(gmg._P_scipy[lv])
+        out[pre + f"P_l{lv}_ij"] = ij
+        out[pre + f"P_l{lv}_v"] = v
+    # one gmg object across the three fields in this order: records the
+    # lambda-cache behaviour (multigrid_v4.py:1175-1188)
+    for tag in ("hi", "mid", "lo"):
+        gmg.setup(fields[tag])
+        out[pre + f"lam_{tag}"] = np.array(gmg.lambda_max_per_level, dtype=np.float64)
+        out[pre + f"omega_{tag}"] = np.array([gmg.omega_used])
+        ap = gmg.adaptive_params
+        out[pre + f"adapt_{tag}"] = np.array(
+            [ap["contrast_ratio"], float(ap["is_high_contrast"]), ap["fine_degree_adapt"],
+             ap["coarse_iters_adapt"]]
+        )
+        if tag == "hi":
+            for lv in range(1, n_levels):
+                ij, v = _coo(gmg._K_gpu[lv])
+                out[pre + f"K_l{lv}_ij"] = ij
+                out[pre + f"K_l{lv}_v"] = v
+            out[pre + "chol_mode"] = np.array([0 if gmg._coarse_chol_mode == "dense" else 1])
+    rhs = rng.standard_normal(len(free))
+    out[pre + "rhs"] = rhs
+    # per-stack preconditioner applies, fresh hierarchy per stack
+    for sname, stack in STACKS.items():
+        for tag in ("hi", "mid"):
+            _, _, _, mf2, g2 = _build(spec, n_levels, stack)
+            g2.setup(fields[tag])
+            out[pre + f"apply_{sname}_{tag}"] = g2.apply(rhs)
+            out[pre + f"lam_{sname}_{tag}"] = np.array(g2.lambda_max_per_level)
+    # node-block Jacobi
+    nb = sv2.NodeBlockJacobiMF(edof, _refshim.load("pub_simp_solver").KE_UNIT_3D, free, len(free), bc.ndof)
+    nb.update(fields["hi"], scalar_diag=mf.extract_diagonal(fields["hi"]))
+    out[pre + "nbj_hi"] = nb.apply(rhs)
+    # full solves (FGMRES, restart 300) for two stacks; PCG for the plain one
+    F = bc.F[free].astype(np.float64)
+    for sname in ("plain_cheb", "canonical", "plain_jacobi"):
+        for variant in ("", "_pert"):
+            _, _, _, mf2, g2 = _build(spec, n_levels, STACKS[sname])
+            E = fields["hi"]
+            if variant:
+                # the reference's own sensitivity: moduli perturbed by 1e-14 relative
+                E = E * (1.0 + 1e-14 * np.random.default_rng(5).standard_normal(E.size))
+            g2.setup(E)
+            hist = []
+            x, it, conv = mg._cupy_fgmres(
+                lambda v: mf2.matvec(v, E), F, g2.apply, tol=1e-6, maxiter=300,
+                restart=300, history=hist,
+            )
+            out[pre + f"fgmres_{sname}{variant}_x"] = x
+            out[pre + f"fgmres_{sname}{variant}_hist"] = np.array(hist)
+            out[pre + f"fgmres_{sname}{variant}_info"] = np.array([it, int(conv), float(F @ x)])
+    for variant in ("", "_pert"):
+        _, _, _, mf2, g2 = _build(spec, n_levels, STACKS["plain_cheb"])
+        E = fields["mid"]
+        if variant:
+            E = E * (1.0 + 1e-14 * np.random.default_rng(5).standard_normal(E.size))
+        g2.setup(E)
+        hist = []
+        x, it, conv = sv2._cupy_pcg(
+            lambda v: mf2.matvec(v, E), F, g2.apply, tol=1e-6, maxiter=200, history=hist,
+        )
+        out[pre + f"pcg_plain{variant}_x"] = x
+        out[pre + f"pcg_plain{variant}_hist"] = np.array(hist)
+        out[pre + f"pcg_plain{variant}_info"] = np.array([it, int(conv), float(F @ x)])
+    _, _, _, mf2, g2 = _build(spec, n_levels, STACKS["plain_cheb"])
+    g2.setup(fields["mid"])
+    # short restarted FGMRES (restart 5) to pin the restart history rule
+    hist = []
+    x, it, conv = mg._cupy_fgmres(
+        lambda v: mf2.matvec(v, fields["mid"]), F, g2.apply, tol=1e-9, maxiter=12, restart=5,
+        history=hist,
+    )
+    out[pre + "fgmres_restart5_x"] = x
+    out[pre + "fgmres_restart5_hist"] = np.array(hist)
+    out[pre + "fgmres_restart5_info"] = np.array([it, int(conv)])
+
+
+def make_policy(tmpdir):
+    """Run the reference prospective driver unchanged on a small preset."""
+    argv = [
+        "--preset", "cantilever_3d", "--probabilities", "0.2,0.35,0.6", "--seeds", "3,5",
+        "--raised-rho-mins", "1e-3,1e-2", "--probe-iters", "30", "--probe-r50", "15",
+        "--maxiter", "60", "--out-dir", tmpdir,
+    ]
+    _refshim.run_driver(
+        os.path.join("experiments", "phase5", "run_gmg_floor_detector_prospective.py"), argv
+    )
+    shutil.copyfile(os.path.join(tmpdir, "prospective_summary.csv"),
+                    os.path.join(HERE, "policy_cantilever_3d_summary.csv"))
+    shutil.copyfile(os.path.join(tmpdir, "prospective_history.csv"),
+                    os.path.join(HERE, "policy_cantilever_3d_history.csv"))
+
+
+def extract_published():
+    root = os.path.join(_refshim.REF_ROOT, "data", "analysis_tables")
+    keep = {
+        "gmg_fixed_floor_controls_strict_true_residual__fixed_floor_control_comparison.csv":
+            "published_fixed_floor_controls.csv",
+        "optimized_density_C512_MF_strict_true_residual__density_detector_summary.csv":
+            "published_C512_MF_summary.csv",
+    }
+    for src, dst in keep.items():
+        shutil.copyfile(os.path.join(root, src), os.path.join(HERE, dst))
+    # held-out cantilever rows used by the quick-start pin (seed 43)
+    src = os.path.join(
+        root, "heldout_gmg_detector_cantilever_s41_71_guarded_true_residual__prospective_summary.csv"
+    )
+    with open(src, newline="") as f:
+        rows = [r for r in csv.DictReader(f) if r["seed"] in ("41", "43")]
+    cols = ["seed", "solid_probability", "probe_r50", "probe_r100", "trigger",
+            "recommended_rho_min", "solve_converged", "solver_reported_converged",
+            "solve_iters", "solve_final_rel_residual", "attempted_rho_mins", "penal"]
+    with open(os.path.join(HERE, "published_heldout_cantilever_s41_s43.csv"), "w", newline="") as f:
+        w = csv.DictWriter(f, fieldnames=cols)
+        w.writeheader()
+        for r in rows:
+            w.writerow({c: r[c] for c in cols})
+    dens = os.path.join(_refshim.REF_ROOT, "data", "optimized_density_inputs")
+    for case in ("C64_MF", "C512_MF"):
+        rho = np.load(os.path.join(dens, f"{case}__rho_final.npy"))
+        np.savez_compressed(os.path.join(HERE, f"density_{case}.npz"), rho=rho)
+
+
+def main():
+    out = {}
+    make_structural(out)
+    for name, (spec, n_levels) in _cases().items():
+        make_case(name, spec, n_levels, out)
+    np.savez_compressed(os.path.join(HERE, "reference_small.npz"), **out)
+    tmp = os.path.join(_refshim.COPY_ROOT, "policy_out")
+    os.makedirs(tmp, exist_ok=True)
+    make_policy(tmp)
+    extract_published()
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main()

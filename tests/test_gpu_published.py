@@ -1,0 +1,97 @@
+"""CUDA path vs the reference's published per-state results and its own driver.
+
+* Fixed-floor controls (data/analysis_tables/gmg_fixed_floor_controls_strict_true_
+  residual__fixed_floor_control_comparison.csv): the canonical stack on the
+  64k cantilever (Bernoulli solid states seed 23 / 31, p = 0.35, and the stored
+  optimized field C64_MF) and on the 512k cantilever (C512_MF), floors
+  1e-12 / 1e-3 / 1e-2 in manifest order through one hierarchy, exactly as
+  experiments/phase5/run_gmg_fixed_floor_controls.py runs them: iteration
+  counts must be identical, compliance within 1e-6 relative, every accepted
+  solve at true relative residual <= 1e-6.
+* The unchanged prospective driver run on cantilever_3d (fixtures made by
+  tests/golden/make_golden.py): trigger, selected floor, attempted floors,
+  convergence flags and iteration counts identical.
+"""
+
+import csv
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _published():
+    with open(os.path.join(GOLDEN, "published_fixed_floor_controls.csv"), newline="") as f:
+        return list(csv.DictReader(f))
+
+
+def _density(case, n_elem):
+    if case.startswith("cant_s"):
+        seed = int(case.split("_")[1][1:])
+        return (np.random.default_rng(seed).random(n_elem) < 0.35).astype(np.float64)
+    rho = np.load(os.path.join(GOLDEN, f"density_{case}.npz"))["rho"].reshape(-1)
+    return np.clip(np.asarray(rho, dtype=np.float64), 0.0, 1.0)
+
+
+def _run_manifest(cuda, preset, cases):
+    from gpu_fem.multigrid_v4 import _cupy_fgmres
+    from gpu_fem.paper4 import CANONICAL_STACK, _build_components
+
+    spec, bc, free, free_gpu, edof, F, mf, gmg = _build_components(preset, n_levels=4, **CANONICAL_STACK)
+    n_elem = spec.nelx * spec.nely * spec.nelz
+    rows = {(r["case_id"], float(r["rho_min"])): r for r in _published()}
+    out = []
+    for case in cases:
+        dens = cuda.as_tensor(_density(case, n_elem), device="cuda")
+        for floor in (1e-12, 1e-3, 1e-2):
+            E = floor + (1.0 - floor) * dens ** 4.5
+            gmg.setup(E)
+            hist = []
+            x, it, conv = _cupy_fgmres(lambda v: mf.matvec(v, E), F, gmg.apply, tol=1e-6, maxiter=300,
+                                       restart=300, history=hist)
+            res = float(cuda.linalg.norm(F - mf.matvec(x, E)) / cuda.linalg.norm(F))
+            compl = float(cuda.dot(F, x))
+            out.append((case, floor, it, compl, res, rows[(case, floor)]))
+    return out
+
+
+def test_fixed_floor_controls_64k(cuda):
+    results = _run_manifest(cuda, "cantilever_gpu_medium", ["cant_s23_p035", "cant_s31_p035", "C64_MF"])
+    for case, floor, it, compl, res, row in results:
+        assert it == int(float(row["solve_iters"])), (case, floor, it, row["solve_iters"])
+        assert abs(compl - float(row["compliance"])) / float(row["compliance"]) <= 1e-6, (case, floor, compl)
+        assert res <= 1e-6
+
+
+def test_fixed_floor_controls_512k(cuda):
+    results = _run_manifest(cuda, "cantilever_gpu_xlarge", ["C512_MF"])
+    for case, floor, it, compl, res, row in results:
+        assert it == int(float(row["solve_iters"])), (case, floor, it, row["solve_iters"])
+        assert abs(compl - float(row["compliance"])) / float(row["compliance"]) <= 1e-6, (case, floor, compl)
+        assert res <= 1e-6
+
+
+def test_prospective_policy_matches_reference_driver(cuda):
+    from gpu_fem.policy import GuardedFloorPolicy
+
+    with open(os.path.join(GOLDEN, "policy_cantilever_3d_summary.csv"), newline="") as f:
+        ref_rows = list(csv.DictReader(f))
+    pol = GuardedFloorPolicy("cantilever_3d", penal=4.5, probe_iters=30, probe_r50=15, maxiter=60,
+                             raised_rho_mins=(1e-3, 1e-2))
+    spec = pol.spec
+    n_elem = spec.nelx * spec.nely * spec.nelz
+    for r in ref_rows:
+        field = np.random.default_rng(int(r["seed"])).random(n_elem)
+        solid = (field < float(r["solid_probability"])).astype(np.float64)
+        out = pol.run(solid, binary=True)
+        assert out["trigger"] == r["trigger"], (r["seed"], r["solid_probability"])
+        assert out["recommended_rho_min"] == float(r["recommended_rho_min"])
+        assert out["attempted_rho_mins"] == r["attempted_rho_mins"]
+        assert out["solve_converged"] == int(r["solve_converged"])
+        assert out["solver_reported_converged"] == int(r["solver_reported_converged"])
+        assert out["solve_iters"] == int(r["solve_iters"])
+        assert abs(out["probe_r50"] - float(r["probe_r50"])) <= 1e-3 * float(r["probe_r50"])

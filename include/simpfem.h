@@ -41,6 +41,9 @@ typedef struct simpfem_gmg simpfem_gmg;
 
 const char* simpfem_last_error(void);
 int simpfem_version(void);
+/* Number of CUDA kernels this library has launched in the process (no reference
+ * counterpart: instrumentation for benchmarks). */
+int64_t simpfem_launch_count(void);
 
 /* Structured hex8 mesh of nelx*nely*nelz unit elements with the given free-DOF
  * list (ascending global DOF indices) and the 24x24 unit element stiffness in
@@ -142,6 +145,12 @@ int simpfem_gmg_setup(simpfem_gmg* g, const double* E, const double* fine_diag_f
 /* z = M(rhs) (GalerkinMatFreeGMG.apply, multigrid_v4.py:1759-1767); FP64 free layout. */
 int simpfem_gmg_apply(simpfem_gmg* g, const double* rhs_free, double* z_free, void* stream);
 int simpfem_gmg_props_get(simpfem_gmg* g, simpfem_gmg_props* out);
+/* Average device time (ms) of one fused smoothing step of `level` (below the
+ * coarsest) -- the operator kernel with the smoother's update fused into its
+ * store, the kernel the cycle launches most -- over `reps` launches timed with CUDA
+ * events on `stream`; clobbers that level's cycle vectors (no reference
+ * counterpart: instrumentation for the roofline report). */
+int simpfem_gmg_time_smoother_step(simpfem_gmg* g, int level, int reps, float* avg_ms, void* stream);
 /* Forget the cached lambda_max estimates (the next setup re-estimates). */
 int simpfem_gmg_reset_lambda_cache(simpfem_gmg* g);
 /* Copy the fine-level operator of the last setup: E as FP64 (n_elem). */

@@ -15,6 +15,16 @@
 
 using namespace simpfem;
 
+#include <atomic>
+static std::atomic<int64_t> g_launches{0};
+namespace simpfem {
+cudaError_t sf_launched(int k) {
+  g_launches.fetch_add(k, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+int64_t sf_launch_count() { return g_launches.load(); }
+}  // namespace simpfem
+
 struct simpfem_mesh {
   Mesh impl;
 };
@@ -50,6 +60,19 @@ extern "C" {
 
 const char* simpfem_last_error(void) { return last_error(); }
 int simpfem_version(void) { return 10000; }
+
+int64_t simpfem_launch_count(void) { return sf_launch_count(); }
+
+int simpfem_gmg_time_smoother_step(simpfem_gmg* g, int level, int reps, float* avg_ms, void* stream) {
+  SF_API_BEGIN
+  if (!g || !avg_ms || reps < 1) throw InvalidArg{"simpfem_gmg_time_smoother_step: invalid argument"};
+  Gmg& G = *g->impl;
+  if (!G.is_setup) throw NotSetup{"GalerkinMatFreeGMG.setup() must be called before apply()."};
+  if (level < 0 || level >= G.L - 1) throw InvalidArg{"simpfem_gmg_time_smoother_step: level out of range"};
+  G.st = S(stream);
+  *avg_ms = time_smoother_step(G, level, reps);
+  SF_API_END
+}
 
 int simpfem_mesh_create(int nelx, int nely, int nelz, const int32_t* free_dofs_host, int64_t n_free,
                         const double* ke_unit_host, simpfem_mesh** out) {

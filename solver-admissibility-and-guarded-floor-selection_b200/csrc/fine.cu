@@ -242,7 +242,7 @@ static cudaError_t launch_sweep(const Grid& g, const SweepShape& sh, const T* E,
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
   dim3 grid(nbj * nbk, div_up(g.nx + 1, sh.cx));
   fine_sweep_kernel<T, EPI, KMODE, MAXT><<<grid, NT, smem, s>>>(g, sh, E, mask, u, ea);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 constexpr int kMaxThreadsF64 = 256;
@@ -322,7 +322,7 @@ __global__ void fine_diag_kernel(Grid g, const double* __restrict__ E, const uin
 cudaError_t launch_fine_diag(const Grid& g, const double* E, const uint8_t* mask, double /*kd*/,
                              double* diag, cudaStream_t s) {
   fine_diag_kernel<<<div_up(g.nn, 256), 256, 0, s>>>(g, E, mask, diag);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -388,7 +388,7 @@ __global__ void node_blocks_kernel(Grid g, const double* __restrict__ E, const u
 cudaError_t launch_node_blocks(const Grid& g, const double* E, const uint8_t* mask,
                                const double* diag_full, double* binv, cudaStream_t s) {
   node_blocks_kernel<<<div_up(g.nn, 256), 256, 0, s>>>(g, E, mask, diag_full, binv);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 __global__ void node_block_apply_kernel(int64_t nn, const double* __restrict__ binv,
@@ -406,7 +406,7 @@ __global__ void node_block_apply_kernel(int64_t nn, const double* __restrict__ b
 cudaError_t launch_node_block_apply(const Grid& g, const double* binv, const double* r, double* z,
                                     const int* guard, cudaStream_t s) {
   node_block_apply_kernel<<<div_up(g.nn, 256), 256, 0, s>>>(g.nn, binv, r, z, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -437,7 +437,7 @@ __global__ void element_energy_kernel(Grid g, const double* __restrict__ u, doub
 
 cudaError_t launch_element_energy(const Grid& g, const double* u_full, double* ce, cudaStream_t s) {
   element_energy_kernel<<<div_up(g.ne(), 256), 256, 0, s>>>(g, u_full, ce);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 }  // namespace simpfem

@@ -20,6 +20,7 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -324,6 +325,9 @@ Gmg* gmg_create(Mesh* m, const simpfem_gmg_opts& o) {
     if (l >= 1) {
       L.K64.alloc(sizeof(double) * 243 * L.g.nn);
       L.dinv64.alloc(sizeof(double) * L.g.ndof);
+      L.s64a.alloc(sizeof(double) * L.g.ndof);
+      L.s64b.alloc(sizeof(double) * L.g.ndof);
+      L.s64c.alloc(sizeof(double) * L.g.ndof);
     }
   }
   // coarsest compact index
@@ -346,6 +350,8 @@ Gmg* gmg_create(Mesh* m, const simpfem_gmg_opts& o) {
     G->cinfo.alloc(16);
   }
   const int64_t n = m->g.ndof;
+  G->Qdev.alloc(8 * m->Q.size());
+  SF_CUDA(cudaMemcpy(G->Qdev.p, m->Q.data(), 8 * m->Q.size(), cudaMemcpyHostToDevice));
   G->E64.alloc(8 * std::max<int64_t>(1, m->g.ne()));
   G->E32.alloc(4 * std::max<int64_t>(1, m->g.ne()));
   G->diag0.alloc(8 * n);
@@ -558,8 +564,8 @@ static void solve_coarsest(Gmg& G, const void* rhs, void* x) {
   }
   if (G.coarse_mode == 1) {
     SF_CUDA(launch_gather_idx(G.nc, G.c_idx.as<int32_t>(), b64, G.cb.as<double>(), G.guard, G.st));
-    SF_CUDA(launch_coarsest_solve(G.Linv.as<double>(), G.nc, G.cb.as<double>(), G.ctmp.as<double>(),
-                                  G.cx.as<double>(), G.guard, G.st));
+    SF_CUDA(launch_coarsest_solve(G.Linv.as<double>(), G.LinvT.as<double>(), G.nc, G.cb.as<double>(),
+                                  G.ctmp.as<double>(), G.cx.as<double>(), G.guard, G.st));
     SF_CUDA(launch_fill(F64, n, 0.0, x64, G.guard, G.st));
     SF_CUDA(launch_scatter_idx(G.nc, G.c_idx.as<int32_t>(), G.cx.as<double>(), x64, G.guard, G.st));
   } else {
@@ -911,6 +917,26 @@ static void fixed_pcg_coarse(Gmg& G, int l, const double* b, double* x) {
 
 // ----------------------------------------------------------------------------
 // setup (multigrid_v4.py:1119-1341)
+struct PhaseTimer {
+  Gmg& G;
+  bool on;
+  std::chrono::steady_clock::time_point t;
+  explicit PhaseTimer(Gmg& g) : G(g), on(getenv("SIMPFEM_TIMING") != nullptr) {
+    if (on) {
+      cudaStreamSynchronize(G.st);
+      t = std::chrono::steady_clock::now();
+    }
+  }
+  void mark(const char* name) {
+    if (!on) return;
+    cudaStreamSynchronize(G.st);
+    auto n = std::chrono::steady_clock::now();
+    fprintf(stderr, "[simpfem setup] %-18s %8.3f ms\n", name,
+            std::chrono::duration<double, std::milli>(n - t).count());
+    t = n;
+  }
+};
+
 static double sync_scalar(Gmg& G, const double* dev) {
   double h;
   SF_CUDA(cudaMemcpyAsync(&h, dev, sizeof(double), cudaMemcpyDeviceToHost, G.st));
@@ -990,13 +1016,9 @@ static double sparse_lambda(Gmg& G, int l) {
   // _estimate_sparse_lambda_max (multigrid_v4.py:389-405), 10 iterations
   Level& L = G.lv[l];
   const int64_t n = L.g.ndof;
-  DevBuf vb, kvb, avb;
-  vb.alloc(8 * n);
-  kvb.alloc(8 * n);
-  avb.alloc(8 * n);
-  double* v = vb.as<double>();
-  double* Kv = kvb.as<double>();
-  double* Av = avb.as<double>();
+  double* v = L.s64a.as<double>();
+  double* Kv = L.s64b.as<double>();
+  double* Av = L.s64c.as<double>();
   const uint8_t* mask = L.mask.as<uint8_t>();
   const double* dinv = L.dinv64.as<double>();
   double* sc = G.m->dscal.as<double>();
@@ -1064,7 +1086,8 @@ static void setup_coarsest(Gmg& G) {
       }
     }
     if (ok) {
-      SF_CUDA(dense_inverse_from_chol(G.Adense.as<double>(), n, G.Linv.as<double>(), nullptr, G.st));
+      G.LinvT.alloc(8 * (size_t)n * n);
+      SF_CUDA(dense_inverse_from_chol(G.Adense.as<double>(), n, G.Linv.as<double>(), G.LinvT.as<double>(), G.st));
       G.coarse_mode = 1;
       return;
     }
@@ -1082,8 +1105,10 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
   const int64_t n = m.g.ndof;
   const int64_t ne = m.g.ne();
   resolve_prec(G);
+  PhaseTimer pt(G);
   if (!m.tuned[0]) tune_mesh(m, F64, G.st);
   if (!m.tuned[1]) tune_mesh(m, F32, G.st);
+  pt.mark("tune");
   SF_CUDA(cudaMemcpyAsync(G.E64.p, E, 8 * ne, cudaMemcpyDeviceToDevice, G.st));
   SF_CUDA(launch_convert(F64, F32, G.E64.p, G.E32.p, ne, nullptr, G.st));
   // diag0 (full layout) and its inverse
@@ -1111,6 +1136,7 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
     SF_CUDA(launch_node_blocks(m.g, G.E64.as<double>(), m.mask.as<uint8_t>(), G.diag0.as<double>(),
                                G.binv.as<double>(), G.st));
   }
+  pt.mark("diag/blocks");
   // lambda cache rule
   G.lam_calls += 1;
   SF_CUDA(launch_minmax_count(ne, G.E64.as<double>(), INFINITY, m.rw, m.dscal.as<double>(), G.st));
@@ -1126,6 +1152,7 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
     G.lam_Emax = Emax;
   }
   G.omega_used = std::min(G.o.omega, 0.9 * 2.0 / std::max(G.lv[0].lam, 1e-6));
+  pt.mark("lambda fine");
   // contrast classification
   G.contrast = Emax / std::max(Emin, 1e-300);
   SF_CUDA(launch_minmax_count(ne, G.E64.as<double>(), Emax * 1e-8, m.rw, m.dscal.as<double>(), G.st));
@@ -1155,19 +1182,17 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
   for (int l = 1; l < G.L; ++l) {
     Level& L = G.lv[l];
     if (l == 1) {
-      DevBuf Qd;
-      Qd.alloc(8 * m.Q.size());
-      SF_CUDA(cudaMemcpyAsync(Qd.p, m.Q.data(), 8 * m.Q.size(), cudaMemcpyHostToDevice, G.st));
-      SF_CUDA(launch_level1_assemble(L.g, m.g, G.E64.as<double>(), Qd.as<double>(), L.mask.as<uint8_t>(),
+      SF_CUDA(launch_level1_assemble(L.g, m.g, G.E64.as<double>(), G.Qdev.as<double>(), L.mask.as<uint8_t>(),
                                      L.K64.as<double>(), G.st));
-      SF_CUDA(cudaStreamSynchronize(G.st));
     } else {
       Level& F = G.lv[l - 1];
       SF_CUDA(launch_rap(F.g, L.g, F.K64.as<double>(), L.mask.as<uint8_t>(), F.wx.as<double>(),
                          F.wy.as<double>(), F.wz.as<double>(), L.K64.as<double>(), G.st));
     }
     SF_CUDA(launch_stencil_diag(L.g, L.K64.as<double>(), L.mask.as<uint8_t>(), L.dinv64.as<double>(), G.st));
+    pt.mark(l == 1 ? "level1 assemble" : "rap");
     if (reest || std::isnan(L.lam)) L.lam = sparse_lambda(G, l);
+    pt.mark("lambda coarse");
     const int p = G.prec[l];
     const bool need32 = (p == F32) || (G.cyc == F32);
     if (need32) {
@@ -1184,7 +1209,9 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
       SF_CUDA(launch_convert(F64, BF16, L.K64.p, L.K16.p, 243 * L.g.nn, nullptr, G.st));
     }
   }
+  pt.mark("precision copies");
   if (G.L > 1) setup_coarsest(G);
+  pt.mark("coarsest");
   SF_CUDA(cudaStreamSynchronize(G.st));
   G.is_setup = true;
 }
@@ -1192,6 +1219,48 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
 }  // namespace simpfem
 
 namespace simpfem {
+
+// Average duration of one smoothing step of `level` in the cycle precision (the
+// kernel the V-cycle launches most), timed with CUDA events on the caller's stream.
+float time_smoother_step(Gmg& G, int l, int reps) {
+  Level& L = G.lv[l];
+  const DType t = G.cyc;
+  const int p = G.prec[l];
+  DType vt = t;
+  if (t == F64 && l == 0 && (p == F32 || p == BF16)) vt = F32;
+  if (t == F64 && l > 0 && p == F32 && L.K32.p) vt = F32;
+  void* x = vt == t ? L.x[0].p : L.xs[0].p;
+  void* xo = vt == t ? L.x[1].p : L.xs[1].p;
+  void* rhs = vt == t ? L.rhs.p : L.rhss.p;
+  void* d = vt == t ? L.d.p : L.ds.p;
+  const size_t es = vt == F64 ? 8 : 4;
+  SF_CUDA(cudaMemsetAsync(x, 0, es * L.g.ndof, G.st));
+  SF_CUDA(cudaMemsetAsync(rhs, 0, es * L.g.ndof, G.st));
+  SF_CUDA(cudaMemsetAsync(d, 0, es * L.g.ndof, G.st));
+  EpiArgs ea;
+  ea.b = rhs;
+  ea.dinv = level_dinv(G, l, vt);
+  ea.d = d;
+  ea.xo = xo;
+  ea.s1 = 0.5;
+  ea.s2 = 0.25;
+  const Epi epi = G.o.smoother_type == 0 ? EPI_CHEB : EPI_JAC;
+  const int psel = (vt == F32) ? p : F64;
+  G.guard = nullptr;
+  level_op(G, l, vt, psel, epi, x, ea);
+  cudaEvent_t e0, e1;
+  SF_CUDA(cudaEventCreate(&e0));
+  SF_CUDA(cudaEventCreate(&e1));
+  SF_CUDA(cudaEventRecord(e0, G.st));
+  for (int r = 0; r < reps; ++r) level_op(G, l, vt, psel, epi, x, ea);
+  SF_CUDA(cudaEventRecord(e1, G.st));
+  SF_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  SF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / reps;
+}
 
 // Outer FGMRES: host-controlled (one synchronisation per iteration to read the
 // device-side convergence flags), history written straight into mapped memory.

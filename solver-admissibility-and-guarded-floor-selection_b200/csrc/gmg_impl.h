@@ -153,6 +153,7 @@ struct Level {
   DevBuf wx, wy, wz;
   // coarse operator (levels >= 1)
   DevBuf K64, K32, K16;
+  DevBuf s64a, s64b, s64c;  // FP64 scratch of the setup-time power iterations
   DevBuf dinv64, dinv32;
   double lam = NAN;
   // cycle vectors in the cycle dtype
@@ -170,7 +171,7 @@ struct Gmg {
   int prec[8];      // resolved per-level smoother precision
   bool prec_resolved = false;
 
-  DevBuf E64, E32, diag0, wenrich, binv;
+  DevBuf E64, E32, diag0, wenrich, binv, Qdev;
   bool is_setup = false;
 
   // lambda cache
@@ -186,7 +187,7 @@ struct Gmg {
   int coarse_mode = 0;
   bool coarse_reg = false;
   int nc = 0;
-  DevBuf c_idx, c_didx, Adense, Linv, cb, cx, ctmp, cinfo;
+  DevBuf c_idx, c_didx, Adense, Linv, LinvT, cb, cx, ctmp, cinfo;
   // iterative coarse (fixed PCG) vectors
   DevBuf pr, pz, pp, pAp;
 
@@ -216,6 +217,7 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free);
 void apply_full(Gmg& G, const double* rhs, double* out, const int* guard);
 void run_outer_fgmres(Gmg& G, const double* b, double* x, bool x0_zero, double tol, int maxiter, int restart,
                       const PrecFn& M, double* hist_dev, int hist_cap);
+float time_smoother_step(Gmg& G, int l, int reps);
 void run_pcg(Gmg& G, const double* b, double* x, double tol, int maxiter, std::vector<double>* hist, int* iters,
              int* conv);
 

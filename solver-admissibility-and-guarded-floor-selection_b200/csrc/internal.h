@@ -180,10 +180,10 @@ cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloo
                               cudaStream_t s);
 
 cudaError_t dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s);
-cudaError_t dense_inverse_from_chol(const double* L, int n, double* Linv, double* work,
+cudaError_t dense_inverse_from_chol(const double* L, int n, double* Linv, double* LinvT,
                                     cudaStream_t s);
-cudaError_t launch_coarsest_solve(const double* Linv, int n, const double* b, double* tmp,
-                                  double* x, const int* guard, cudaStream_t s);
+cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b,
+                                  double* tmp, double* x, const int* guard, cudaStream_t s);
 cudaError_t launch_add_diag(double* A, int n, double eps, cudaStream_t s);
 cudaError_t launch_diag_sum(const double* A, int n, double* out, cudaStream_t s);
 cudaError_t launch_all_finite(const double* A, int64_t n, int* flag, cudaStream_t s);
@@ -219,6 +219,10 @@ cudaError_t launch_dmul(int64_t n, const double* dinv, const double* r, double* 
                         cudaStream_t s);
 cudaError_t launch_select_vec(DType t, int64_t n, const void* trial, const void* r,
                               const double* sc, void* out, const int* guard, cudaStream_t s);
+
+// launch accounting: every launcher reports its kernel launches here
+cudaError_t sf_launched(int k);
+int64_t sf_launch_count();
 
 // error plumbing
 void set_error(const std::string& msg);

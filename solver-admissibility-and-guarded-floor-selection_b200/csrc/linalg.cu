@@ -114,7 +114,7 @@ cudaError_t launch_dots(DType t, int64_t n, const DotSet& ds, RedWork w, double*
     return cudaErrorInvalidValue;
   }
 #undef SF_DOTS
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // min, max and count(E > thr) of a double array (contrast classification,
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kRedThreads) minmax_kernel(int64_t n, const do
 cudaError_t launch_minmax_count(int64_t n, const double* E, double thr, RedWork w, double* out3,
                                 cudaStream_t s) {
   minmax_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(n, E, thr, w, out3);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -210,7 +210,7 @@ cudaError_t launch_axpby(DType t, int64_t n, double alpha, const void* x, double
   else
     axpby_kernel<float><<<nb, 256, 0, s>>>(n, (float)alpha, (const float*)x, (float)beta,
                                            (const float*)y, (float*)out, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 template <typename T>
@@ -226,7 +226,7 @@ cudaError_t launch_fill(DType t, int64_t n, double v, void* out, const int* guar
     fill_kernel<double><<<nb, 256, 0, s>>>(n, v, (double*)out, guard);
   else
     fill_kernel<float><<<nb, 256, 0, s>>>(n, (float)v, (float*)out, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 cudaError_t launch_copy(DType t, int64_t n, const void* src, void* dst, const int* guard,
@@ -256,7 +256,7 @@ cudaError_t launch_cheb_zero(DType t, int64_t n, double alpha, const void* dinv,
   else
     cheb_zero_kernel<float><<<nb, 256, 0, s>>>(n, (float)alpha, (const float*)dinv,
                                                (const float*)rhs, (float*)d, (float*)x, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // First damped-Jacobi step from x0 = 0: x = (omega * dinv) * rhs.
@@ -278,7 +278,7 @@ cudaError_t launch_jac_zero(DType t, int64_t n, double omega, const void* dinv, 
   else
     jac_zero_kernel<float><<<nb, 256, 0, s>>>(n, (float)omega, (const float*)dinv,
                                               (const float*)rhs, (float*)x, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 template <typename T>
@@ -301,7 +301,7 @@ cudaError_t launch_expand(DType t, int64_t n_free, const int32_t* free_idx, cons
     expand_kernel<double><<<nb, 256, 0, s>>>(n_free, free_idx, (const double*)src_free, (double*)dst_full);
   else
     expand_kernel<float><<<nb, 256, 0, s>>>(n_free, free_idx, (const float*)src_free, (float*)dst_full);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 cudaError_t launch_compress(DType t, int64_t n_free, const int32_t* free_idx,
@@ -311,7 +311,7 @@ cudaError_t launch_compress(DType t, int64_t n_free, const int32_t* free_idx,
     compress_kernel<double><<<nb, 256, 0, s>>>(n_free, free_idx, (const double*)src_full, (double*)dst_free);
   else
     compress_kernel<float><<<nb, 256, 0, s>>>(n_free, free_idx, (const float*)src_full, (float*)dst_free);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 __global__ void gather_idx_kernel(int64_t n, const int32_t* __restrict__ idx, const double* __restrict__ src,
@@ -330,12 +330,12 @@ __global__ void scatter_idx_kernel(int64_t n, const int32_t* __restrict__ idx, c
 cudaError_t launch_gather_idx(int64_t n, const int32_t* idx, const double* src, double* dst,
                               const int* guard, cudaStream_t s) {
   gather_idx_kernel<<<div_up(n, 256), 256, 0, s>>>(n, idx, src, dst, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 cudaError_t launch_scatter_idx(int64_t n, const int32_t* idx, const double* src, double* dst,
                                const int* guard, cudaStream_t s) {
   scatter_idx_kernel<<<div_up(n, 256), 256, 0, s>>>(n, idx, src, dst, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // out = mask ? op(a) : 0 with
@@ -367,7 +367,7 @@ __global__ void vec_op_kernel(int64_t n, int op, const double* __restrict__ a, c
 cudaError_t launch_vec_op(int64_t n, int op, const double* a, const double* b, const uint8_t* mask,
                           double s, const double* s_dev, double* out, cudaStream_t st) {
   vec_op_kernel<<<div_up(n, 256), 256, 0, st>>>(n, op, a, b, mask, s, s_dev, out);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // Root-enrichment weights (gpu_fem/multigrid_v4.py:1150-1157):
@@ -391,7 +391,7 @@ cudaError_t launch_enrich_weights(int64_t n, const double* diag, const uint8_t* 
                                   const double* dmax_dev, double wfloor, double wpow, double* w,
                                   cudaStream_t s) {
   enrich_weight_kernel<<<div_up(n, 256), 256, 0, s>>>(n, diag, mask, dmax_dev, wfloor, wpow, w);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // out = mask ? (mode 0: w * r ; mode 1: clip(1 - w, floor, 1) * r ;
@@ -417,7 +417,7 @@ cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloo
                               const double* p, const uint8_t* mask, double* out, const int* guard,
                               cudaStream_t s) {
   enrich_rhs_kernel<<<div_up(n, 256), 256, 0, s>>>(n, mode, w, wfloor, r, p, mask, out, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -508,89 +508,139 @@ cudaError_t dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s) {
   cudaMemsetAsync(info_dev, 0, sizeof(int), s);
   for (int k0 = 0; k0 < n; k0 += NB) {
     potrf_diag_kernel<<<1, 256, 0, s>>>(A, n, k0, info_dev);
+    sf_launched(1);
     const int kb = std::min(NB, n - k0);
     const int rest = n - k0 - kb;
     if (rest > 0) {
       trsm_panel_kernel<<<div_up(rest, 128), 128, 0, s>>>(A, n, k0);
       const int nt = div_up(rest, NB);
       syrk_update_kernel<<<dim3(nt, nt), 256, 0, s>>>(A, n, k0);
+      sf_launched(2);
     }
   }
-  // zero the strict upper triangle so the factor is a clean lower matrix
   return cudaGetLastError();
 }
 
-// Linv = L^{-1}: block of 32 columns per CTA, forward substitution row by row.
-__global__ void tri_inverse_kernel(const double* __restrict__ L, int n, double* __restrict__ Linv) {
-  const int c0 = blockIdx.x * NB;
-  const int cb = min(NB, n - c0);
-  const int col = threadIdx.x & (NB - 1);   // 32 columns
-  const int part = threadIdx.x >> 5;        // 8 partial sums per column
-  const int nparts = blockDim.x >> 5;
-  __shared__ double red[8][NB];
-  // rows < c0 are zero
-  for (int r = c0; r < n; ++r) {
-    double s = 0.0;
-    if (col < cb) {
-      for (int j = c0 + part; j < r; j += nparts) s += L[(int64_t)r * n + j] * Linv[(int64_t)j * n + c0 + col];
-    }
-    red[part][col] = s;
-    __syncthreads();
-    if (part == 0 && col < cb) {
-      double t = 0.0;
-      for (int p = 0; p < nparts; ++p) t += red[p][col];
-      const double e = (r == c0 + col) ? 1.0 : 0.0;
-      Linv[(int64_t)r * n + c0 + col] = (r < c0 + col) ? 0.0 : (e - t) / L[(int64_t)r * n + r];
-    }
-    __syncthreads();
+// Linv = L^{-1} by 32x32 blocks: diagonal blocks inverted independently, then
+// the off-diagonal blocks one block-diagonal at a time,
+//   Linv_ik = -Linv_ii * sum_{j=k}^{i-1} L_ij Linv_jk   (i - k = d),
+// every block of one block-diagonal in parallel.
+__global__ void diag_block_inverse_kernel(const double* __restrict__ L, int n, double* __restrict__ Li) {
+  __shared__ double T[NB][NB + 1];
+  __shared__ double X[NB][NB + 1];
+  const int k0 = blockIdx.x * NB;
+  const int kb = min(NB, n - k0);
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    T[r][c] = (r < kb && c < kb) ? L[(int64_t)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
   }
-}
-
-cudaError_t dense_inverse_from_chol(const double* L, int n, double* Linv, double* /*work*/,
-                                    cudaStream_t s) {
-  cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, s);
-  tri_inverse_kernel<<<div_up(n, NB), 256, 0, s>>>(L, n, Linv);
-  return cudaGetLastError();
-}
-
-// t = Linv b (warp per row) ; x = Linv^T t (thread per column)
-__global__ void trmv_lower_kernel(const double* __restrict__ Li, int n, const double* __restrict__ b,
-                                  double* __restrict__ t, const int* guard) {
-  if (guard_off(guard)) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  double s = 0.0;
-  const double* row = Li + (int64_t)warp * n;
-  for (int j = lane; j <= warp; j += 32) s += row[j] * b[j];
-  s = warp_sum(s);
-  if (lane == 0) t[warp] = s;
-}
-
-__global__ void trmv_lowerT_kernel(const double* __restrict__ Li, int n, const double* __restrict__ t,
-                                   double* __restrict__ x, const int* guard) {
-  if (guard_off(guard)) return;
-  // block of 32 columns x 8 row-slices, reduced in shared memory
-  const int col = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int part = threadIdx.x >> 5;
-  __shared__ double red[8][32];
-  double s = 0.0;
-  if (col < n)
-    for (int i = col + part; i < n; i += 8) s += Li[(int64_t)i * n + col] * t[i];
-  red[part][threadIdx.x & 31] = s;
   __syncthreads();
-  if (part == 0 && col < n) {
-    double a = 0.0;
-    for (int p = 0; p < 8; ++p) a += red[p][threadIdx.x & 31];
-    x[col] = a;
+  // column c of X solves T x = e_c by forward substitution, one thread per column
+  if (threadIdx.x < NB) {
+    const int c = threadIdx.x;
+    for (int r = 0; r < NB; ++r) {
+      double a = (r == c) ? 1.0 : 0.0;
+      for (int p = c; p < r; ++p) a -= T[r][p] * X[p][c];
+      X[r][c] = (r < c) ? 0.0 : a / T[r][r];
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    if (r < kb && c < kb) Li[(int64_t)(k0 + r) * n + k0 + c] = X[r][c];
   }
 }
 
-cudaError_t launch_coarsest_solve(const double* Linv, int n, const double* b, double* tmp,
+__global__ void offdiag_inverse_kernel(const double* __restrict__ L, int n, int d, double* __restrict__ Li) {
+  const int k = blockIdx.x;
+  const int i = k + d;
+  const int i0 = i * NB, k0 = k * NB;
+  const int ib = min(NB, n - i0), kb = min(NB, n - k0);
+  __shared__ double A[NB][NB + 1], B[NB][NB + 1];
+  const int tr = threadIdx.x / NB;  // 0..7 (256 threads)
+  const int tc = threadIdx.x % NB;
+  double acc[4] = {0, 0, 0, 0};
+  for (int j = k; j < i; ++j) {
+    const int j0 = j * NB;
+    const int jb = min(NB, n - j0);
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+      const int r = idx / NB, c = idx % NB;
+      A[r][c] = (r < ib && c < jb) ? L[(int64_t)(i0 + r) * n + j0 + c] : 0.0;
+      B[r][c] = (r < jb && c < kb) ? Li[(int64_t)(j0 + r) * n + k0 + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = tr + 8 * q;
+#pragma unroll 8
+      for (int p = 0; p < NB; ++p) acc[q] += A[r][p] * B[p][tc];
+    }
+    __syncthreads();
+  }
+  // Li_ik = -Li_ii * acc
+  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx / NB, c = idx % NB;
+    A[r][c] = (r < ib && c < ib) ? Li[(int64_t)(i0 + r) * n + i0 + c] : 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) B[tr + 8 * q][tc] = acc[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = tr + 8 * q;
+    double s = 0.0;
+    for (int p = 0; p <= r; ++p) s += A[r][p] * B[p][tc];
+    if (r < ib && tc < kb) Li[(int64_t)(i0 + r) * n + k0 + tc] = -s;
+  }
+}
+
+__global__ void transpose_kernel(const double* __restrict__ A, int n, double* __restrict__ At) {
+  __shared__ double T[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = by + r, j = bx + threadIdx.x;
+    T[r][threadIdx.x] = (i < n && j < n) ? A[(int64_t)i * n + j] : 0.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = bx + r, j = by + threadIdx.x;
+    if (i < n && j < n) At[(int64_t)i * n + j] = T[threadIdx.x][r];
+  }
+}
+
+// Linv (lower) and LinvT (its transpose, upper) from the Cholesky factor L.
+cudaError_t dense_inverse_from_chol(const double* L, int n, double* Linv, double* LinvT, cudaStream_t s) {
+  cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, s);
+  const int nb = div_up(n, NB);
+  diag_block_inverse_kernel<<<nb, 64, 0, s>>>(L, n, Linv);
+  for (int d = 1; d < nb; ++d) offdiag_inverse_kernel<<<nb - d, 256, 0, s>>>(L, n, d, Linv);
+  transpose_kernel<<<dim3(nb, nb), dim3(32, 8), 0, s>>>(Linv, n, LinvT);
+  return sf_launched(nb + 1);
+}
+
+// y = M b over the triangle of a dense row-major M (lower: j <= i, upper: j >= i),
+// one warp per row.
+template <int UPPER>
+__global__ void tri_matvec_kernel(const double* __restrict__ M, int n, const double* __restrict__ b,
+                                  double* __restrict__ y, const int* guard) {
+  if (guard_off(guard)) return;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const double* r = M + (int64_t)row * n;
+  const int lo = UPPER ? row : 0, hi = UPPER ? n : row + 1;
+  double s = 0.0;
+  for (int j = lo + lane; j < hi; j += 32) s += r[j] * b[j];
+  s = warp_sum(s);
+  if (lane == 0) y[row] = s;
+}
+
+cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b, double* tmp,
                                   double* x, const int* guard, cudaStream_t s) {
-  trmv_lower_kernel<<<div_up((int64_t)n * 32, 256), 256, 0, s>>>(Linv, n, b, tmp, guard);
-  trmv_lowerT_kernel<<<div_up(n, 32), 256, 0, s>>>(Linv, n, tmp, x, guard);
-  return cudaGetLastError();
+  const int blocks = div_up((int64_t)n * 32, 256);
+  tri_matvec_kernel<0><<<blocks, 256, 0, s>>>(Linv, n, b, tmp, guard);
+  tri_matvec_kernel<1><<<blocks, 256, 0, s>>>(LinvT, n, tmp, x, guard);
+  return sf_launched(2);
 }
 
 __global__ void add_diag_kernel(double* A, int n, double eps) {
@@ -599,7 +649,7 @@ __global__ void add_diag_kernel(double* A, int n, double eps) {
 }
 cudaError_t launch_add_diag(double* A, int n, double eps, cudaStream_t s) {
   add_diag_kernel<<<div_up(n, 256), 256, 0, s>>>(A, n, eps);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 __global__ void diag_sum_kernel(const double* A, int n, double* out) {
@@ -618,7 +668,7 @@ __global__ void diag_sum_kernel(const double* A, int n, double* out) {
 }
 cudaError_t launch_diag_sum(const double* A, int n, double* out, cudaStream_t s) {
   diag_sum_kernel<<<1, 256, 0, s>>>(A, n, out);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 __global__ void all_finite_kernel(const double* A, int64_t n, int* flag) {
@@ -627,7 +677,7 @@ __global__ void all_finite_kernel(const double* A, int64_t n, int* flag) {
 }
 cudaError_t launch_all_finite(const double* A, int64_t n, int* flag, cudaStream_t s) {
   all_finite_kernel<<<div_up(n, 256), 256, 0, s>>>(A, n, flag);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -668,7 +718,7 @@ cudaError_t launch_mgs_step(int64_t n, const double* vi, const double* vnext, do
                             const double* hi, RedWork rw, double* out, const int* guard,
                             cudaStream_t s) {
   mgs_step_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(n, vi, vnext, w, hi, rw, out, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // Krylov control (single thread).  Flags: see KrylovDev in internal.h.
@@ -773,7 +823,7 @@ __global__ void scale_vec_kernel(int64_t n, const double* __restrict__ src, cons
 cudaError_t launch_scale_vec(int64_t n, const double* src, const double* denom_dev, double* dst,
                              const int* guard, cudaStream_t s) {
   scale_vec_kernel<<<div_up(n, 256), 256, 0, s>>>(n, src, denom_dev, dst, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // Back substitution R y = g[:jf] (column-oriented, R = triu(H[:jf, :jf])).
@@ -800,7 +850,7 @@ __global__ void backsolve_kernel(KrylovDev k) {
 
 cudaError_t launch_backsolve(KrylovDev k, cudaStream_t s) {
   backsolve_kernel<<<1, 256, 0, s>>>(k);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // x <- x + y_0 Z_0 + y_1 Z_1 + ... (sequential per element, as the reference's loop)
@@ -818,7 +868,7 @@ __global__ void update_x_kernel(int64_t n, double* __restrict__ x, double* const
 cudaError_t launch_update_x(int64_t n, double* x, double* const* Z_dev, const double* y,
                             const int* flags, cudaStream_t s) {
   update_x_kernel<<<div_up(n, 256), 256, 0, s>>>(n, x, Z_dev, y, flags);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -861,7 +911,7 @@ __global__ void scalar_op_kernel(int op, double* sc, double p0, double p1, const
 cudaError_t launch_scalar_op(int op, double* sc, double p0, double p1, const int* guard,
                              cudaStream_t s) {
   scalar_op_kernel<<<1, 1, 0, s>>>(op, sc, p0, p1, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // x <- accept ? x + s * c : x   (s = 1 uses x + c)
@@ -884,7 +934,7 @@ cudaError_t launch_select_axpy(DType t, int64_t n, void* x, const void* c, const
   else
     select_axpy_kernel<float><<<div_up(n, 256), 256, 0, s>>>(n, (float*)x, (const float*)c, sc,
                                                              unit, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // trial = r - s * Ac (s from sc[4], or 1 when unit) ; sc[5] = |trial|^2
@@ -916,7 +966,7 @@ cudaError_t launch_trial_residual(DType t, int64_t n, const void* r, const void*
   else
     trial_kernel<float><<<red_blocks(n), kRedThreads, 0, s>>>(n, (const float*)r, (const float*)Ac, sc,
                                                               unit, (float*)trial, rw, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // Select between the accepted trial residual and the old residual:
@@ -938,22 +988,22 @@ cudaError_t launch_select_vec(DType t, int64_t n, const void* trial, const void*
   else
     select_vec_kernel<float><<<div_up(n, 256), 256, 0, s>>>(n, (const float*)trial, (const float*)r,
                                                             sc, (float*)out, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 cudaError_t launch_krylov_init(KrylovDev k, const int* parent, cudaStream_t s) {
   krylov_init_kernel<<<1, 1, 0, s>>>(k, parent);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 cudaError_t launch_krylov_restart(KrylovDev k, double tol, double* hist_host, int hist_cap,
                                   cudaStream_t s) {
   krylov_restart_kernel<<<1, 1, 0, s>>>(k, tol, hist_host, hist_cap);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 cudaError_t launch_givens(KrylovDev k, int j, double tol, double* hist_host, int hist_cap,
                           cudaStream_t s) {
   givens_kernel<<<1, 1, 0, s>>>(k, j, tol, hist_host, hist_cap);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -971,7 +1021,7 @@ __global__ void pcg_scalar_kernel(int which, double* sc, const int* guard) {
 
 cudaError_t launch_pcg_scalar(int which, double* sc, const int* guard, cudaStream_t s) {
   pcg_scalar_kernel<<<1, 1, 0, s>>>(which, sc, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // x += alpha p ; r -= alpha Ap ; z = dinv r ; sc[2] = <r, z>
@@ -1001,7 +1051,7 @@ __global__ void __launch_bounds__(kRedThreads) pcg_xr_kernel(int64_t n, double* 
 cudaError_t launch_pcg_xr(int64_t n, double* x, double* r, double* z, const double* p, const double* Ap,
                           const double* dinv, double* sc, RedWork rw, const int* guard, cudaStream_t s) {
   pcg_xr_kernel<<<red_blocks(n), kRedThreads, 0, s>>>(n, x, r, z, p, Ap, dinv, sc, rw, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // p = z + beta p
@@ -1015,7 +1065,7 @@ __global__ void pcg_p_kernel(int64_t n, const double* __restrict__ z, double* __
 cudaError_t launch_pcg_p(int64_t n, const double* z, double* p, const double* sc, const int* guard,
                          cudaStream_t s) {
   pcg_p_kernel<<<div_up(n, 256), 256, 0, s>>>(n, z, p, sc, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // z = dinv * r (elementwise), guarded
@@ -1029,7 +1079,7 @@ __global__ void dmul_kernel(int64_t n, const double* __restrict__ dinv, const do
 cudaError_t launch_dmul(int64_t n, const double* dinv, const double* r, double* z, const int* guard,
                         cudaStream_t s) {
   dmul_kernel<<<div_up(n, 256), 256, 0, s>>>(n, dinv, r, z, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 }  // namespace simpfem

@@ -70,7 +70,7 @@ static cudaError_t stencil_dispatch(Epi epi, const Grid& g, const void* coef, co
     case EPI_JAC: stencil_kernel<VT, CT, EPI_JAC><<<nb, bs, 0, s>>>(g, c, mask, uu, ea); break;
     default: return cudaErrorInvalidValue;
   }
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 cudaError_t launch_stencil(DType vt, DType ct, Epi epi, const Grid& g, const void* coef,
@@ -145,7 +145,7 @@ cudaError_t launch_level1_assemble(const Grid& gc, const Grid& gf, const double*
                                    const double* Q, const uint8_t* mask_c, double* coef,
                                    cudaStream_t s) {
   level1_assemble_kernel<<<div_up(27 * gc.nn, 128), 128, 0, s>>>(gc, gf, E_fine, Q, mask_c, coef);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -204,7 +204,7 @@ cudaError_t launch_rap(const Grid& gf, const Grid& gc, const double* coef_f, con
                        const double* wx, const double* wy, const double* wz, double* coef_c,
                        cudaStream_t s) {
   rap_kernel<<<div_up(27 * gc.nn, 128), 128, 0, s>>>(gf, gc, coef_f, mask_c, wx, wy, wz, coef_c);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 __global__ void stencil_diag_kernel(Grid g, const double* __restrict__ coef, const uint8_t* __restrict__ mask,
@@ -221,7 +221,7 @@ __global__ void stencil_diag_kernel(Grid g, const double* __restrict__ coef, con
 cudaError_t launch_stencil_diag(const Grid& g, const double* coef, const uint8_t* mask,
                                 double* dinv, cudaStream_t s) {
   stencil_diag_kernel<<<div_up(g.ndof, 256), 256, 0, s>>>(g, coef, mask, dinv);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -282,7 +282,7 @@ cudaError_t launch_restrict(DType t, const Grid& gf, const Grid& gc, const doubl
   else
     restrict_kernel<float><<<nb, 128, 0, s>>>(gf, gc, wx, wy, wz, mask_c, (const float*)fine,
                                               (float*)coarse, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 cudaError_t launch_prolong(DType t, const Grid& gf, const Grid& gc, const double* wx,
@@ -295,7 +295,7 @@ cudaError_t launch_prolong(DType t, const Grid& gf, const Grid& gc, const double
   else
     prolong_kernel<float><<<nb, 128, 0, s>>>(gf, gc, wx, wy, wz, mask_f, (const float*)coarse,
                                              (float*)fine, guard);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -329,7 +329,7 @@ cudaError_t launch_stencil_to_dense(const Grid& g, const double* coef, const int
   cudaError_t e = cudaMemsetAsync(A, 0, sizeof(double) * n * n, s);
   if (e != cudaSuccess) return e;
   stencil_to_dense_kernel<<<div_up(27 * g.ndof, 256), 256, 0, s>>>(g, coef, dense_idx, n, A);
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 // ----------------------------------------------------------------------------
@@ -364,7 +364,7 @@ cudaError_t launch_convert(DType from, DType to, const void* src, void* dst, int
     convert_kernel<float, float><<<nb, 256, 0, s>>>((const float*)src, (float*)dst, n, guard);
   else
     return cudaErrorInvalidValue;
-  return cudaGetLastError();
+  return sf_launched(1);
 }
 
 }  // namespace simpfem

@@ -1,0 +1,98 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports every
+entry point include/simpfem.h declares; the Python layer's boundary inputs
+(KE, edof, presets, BCs) match the reference; argument validation raises the
+reference's errors; the policy's classification rule."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    with open(os.path.join(ROOT, "include", "simpfem.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(simpfem_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from gpu_fem import _lib
+
+    lib = _lib.load()
+    declared = _declared()
+    assert declared, "no declarations found"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) == set(_lib.exported_symbols())
+    assert lib.simpfem_version() >= 10000
+
+
+def test_element_data_and_bcs(ref):
+    from gpu_fem import presets
+    from gpu_fem.bc_generator import generate_bc
+    from gpu_fem.pub_simp_solver import KE_UNIT_3D, _build_density_filter, _edof_table_3d
+
+    assert np.abs(KE_UNIT_3D - ref["KE_UNIT_3D"]).max() <= 1e-15
+    assert np.array_equal(_edof_table_3d(3, 2, 2), ref["edof_3x2x2"])
+    assert np.abs(_build_density_filter(6, 4, 1.5, 3).toarray() - ref["filter_643_r15"]).max() <= 1e-15
+    for name, spec in (("cant24", presets.get_preset("cantilever_3d")), ("bridge30", presets.get_preset("bridge_3d")),
+                       ("odd13", presets.cantilever_spec(13, 7, 5))):
+        bc = generate_bc(spec)
+        assert np.array_equal(bc.free_dofs, ref[f"{name}/free"])
+        assert np.abs(bc.F - ref[f"{name}/F"]).max() == 0.0
+    with pytest.raises(KeyError):
+        presets.get_preset("no_such_preset")
+
+
+def test_grid_from_edof():
+    from gpu_fem._native import grid_from_edof
+    from gpu_fem.pub_simp_solver import _edof_table_3d
+
+    assert grid_from_edof(_edof_table_3d(7, 3, 5)) == (7, 3, 5)
+    bad = _edof_table_3d(4, 3, 2).copy()
+    bad[5, 0] += 3
+    with pytest.raises(ValueError):
+        grid_from_edof(bad)
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(smoother_type="sor"), "smoother_type must be"),
+    (dict(cycle_type="f"), "cycle_type must be"),
+    (dict(coarse_correction_policy="x"), "coarse_correction_policy must be"),
+    (dict(coarse_correction_acceptance_ratio=0.0), "coarse_correction_acceptance_ratio must be positive"),
+    (dict(root_enrichment_mode="x"), "root_enrichment_mode must be"),
+    (dict(root_enrichment_weight_floor=0.0), "root_enrichment_weight_floor must lie"),
+    (dict(root_local_correction_mode="x"), "root_local_correction_mode must be"),
+    (dict(root_local_correction_inner_steps=0), "root_local_correction_inner_steps must be positive"),
+    (dict(inner_krylov_steps=-1), "inner_krylov_steps must be non-negative"),
+    (dict(inner_krylov_restart=0), "inner_krylov_restart must be positive"),
+])
+def test_gmg_option_validation(kw, msg):
+    from gpu_fem.multigrid_v4 import GalerkinMatFreeGMG
+
+    with pytest.raises(ValueError, match=msg):
+        GalerkinMatFreeGMG(mf_op=None, free=np.arange(3), free_gpu=None, nelx=2, nely=2, nelz=2, KE_UNIT=None, **kw)
+
+
+def test_classify_rule():
+    from gpu_fem.policy import _classify
+
+    th = dict(high_residual_threshold=1e-2, plateau_residual_threshold=1e-4, plateau_ratio_threshold=0.6)
+    assert _classify(2e-2, 1e-6, **th) == (True, "high_r50")
+    assert _classify(5e-4, 4e-4, **th) == (True, "plateau")
+    assert _classify(5e-4, 1e-4 * 0.5, **th) == (False, "keep")
+    assert _classify(1e-3, 5e-4, **th) == (False, "keep")   # ratio 0.5 < 0.6
+
+
+def test_ops_refuse_without_gpu():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from gpu_fem import _lib
+
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        _lib.require_cuda()

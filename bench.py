@@ -1,0 +1,355 @@
+"""Benchmark: guarded solves/s to true relative residual 1e-6 on the 512k-element
+cantilever (160 x 80 x 40), mixed precision vs FP64, one B200 per rank.
+
+A step is one guarded solve of one state: probe at rho_min = 1e-12, r50/r100
+preserve/escalate rule, floor ladder {1e-12 | 1e-3, 1e-2}, FP64 recomputed
+true-residual guard (gpu_fem.policy.GuardedFloorPolicy).  States follow the
+synthetic generator of the workload: element void with probability
+p in {0.2, 0.35, 0.5} (seeded Bernoulli), otherwise solid, cone filter of
+radius 1.5, E = 1e-12 + (1 - 1e-12) rho_f^3, unit tip load, x = 0 face clamped.
+The hierarchy is the damped-Jacobi V-cycle (4 levels, FGMRES restart 300,
+tol 1e-6); ``--stack canonical`` selects the reference drivers' default stack.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
+
+N > 1 (torchrun): ranks solve disjoint states, no collective on the data path;
+the reported value is all states / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "solver-admissibility-and-guarded-floor-selection_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 160, 80, 40
+PROBS = (0.2, 0.35, 0.5)
+METRIC = "guarded solves/s & s/solve to true resid 1e-6 @512k elems: mixed vs FP64, 1 B200"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--stack", default="plain", choices=["plain", "canonical"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _filter():
+    from oracle.solver import density_filter
+
+    return density_filter(NX, NY, NZ, 1.5)
+
+
+def make_state(H, seed: int) -> np.ndarray:
+    p = PROBS[seed % len(PROBS)]
+    solid = (np.random.default_rng(seed).random(NX * NY * NZ) >= p).astype(np.float64)
+    return np.asarray(H @ solid)
+
+
+def _stack(name: str, precision: str) -> dict:
+    from gpu_fem.paper4 import CANONICAL_STACK, PLAIN_JACOBI_STACK
+
+    st = dict(CANONICAL_STACK if name == "canonical" else PLAIN_JACOBI_STACK)
+    st["fine_smoother"] = "fp32" if precision == "mixed" else "fp64"
+    return st
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in out.stdout.strip().split(",")]
+                if len(f) >= 7:
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(s[0]) for s in self.samples) if v is not None]
+        mx = [v for v in (num(s[1]) for s in self.samples) if v is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_per_launch():
+    """DRAM bytes per launch of the timed kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def run_native(args):
+    import torch
+    import torch.distributed as dist
+
+    from gpu_fem import _lib
+    from gpu_fem.policy import GuardedFloorPolicy
+    from gpu_fem.presets import cantilever_spec
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+    H = _filter()
+    spec = cantilever_spec(NX, NY, NZ)
+    K, W = args.steps, args.warmup
+    seeds = [1000 * rank + i for i in range(W + 2 * K)]
+    states = {s: make_state(H, s) for s in seeds}
+
+    def policy(precision):
+        return GuardedFloorPolicy(spec, penal=3.0, tol=1e-6, restart=300, maxiter=300, probe_iters=100,
+                                  probe_r50=50, raised_rho_mins=(1e-3, 1e-2), stack=_stack(args.stack, precision),
+                                  cycle_precision="fp32" if precision == "mixed" else "fp64")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(pol, seq, host_io: bool):
+        dev = {s: torch.as_tensor(states[s], device="cuda") for s in seq} if not host_io else None
+        host = {s: torch.as_tensor(states[s]).pin_memory() for s in seq} if host_io else None
+        rows = []
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = _lib.lib().simpfem_launch_count()
+        e0.record()
+        for s in seq:
+            if host_io:
+                out = pol.run(host[s].to("cuda", non_blocking=True))
+                out["x_host"] = pol.last_x.to("cpu")
+            else:
+                out = pol.run(dev[s])
+            rows.append(out)
+        e1.record()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        launches = _lib.lib().simpfem_launch_count() - l0
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, rows, launches
+
+    mixed = policy("mixed")
+    for s in seeds[:W]:
+        mixed.run(torch.as_tensor(states[s], device="cuda"))
+    timed_seeds = seeds[W:W + K]
+    with ClockSampler(local) as clk:
+        ms_mixed, rows_mixed, launches = timed(mixed, timed_seeds, host_io=False)
+    ms_e2e, rows_e2e, _ = timed(mixed, seeds[W + K:W + 2 * K], host_io=True)
+    # FP64 from-scratch comparison on the same states
+    fp64 = policy("fp64")
+    for s in seeds[:W]:
+        fp64.run(torch.as_tensor(states[s], device="cuda"))
+    ms_fp64, rows_fp64, _ = timed(fp64, timed_seeds, host_io=False)
+
+    n_states = K * world
+    value = n_states / (ms_mixed / 1e3)
+    e2e_value = n_states / (ms_e2e / 1e3)
+    n_free = int(mixed.F_free_gpu.numel())
+
+    # roofline of the dominant kernel: the fused fine smoothing step of the cycle
+    hbm_peak, peak_kind = _peaks()
+    avg = ctypes.c_float()
+    _lib.call("simpfem_gmg_time_smoother_step", mixed.gmg._h, 0, 50, ctypes.byref(avg), _lib.stream_ptr())
+    ndof = 3 * (NX + 1) * (NY + 1) * (NZ + 1)
+    ne = NX * NY * NZ
+    # fp32 vectors read u, rhs, dinv (plus d for Chebyshev) and write x (plus d); E (fp32); 1-byte DOF mask
+    nvec = 4 if args.stack == "plain" else 6
+    alg_bytes = nvec * 4 * ndof + 4 * ne + ndof
+    achieved = alg_bytes / (avg.value * 1e-3) / 1e9
+    traffic = _traffic_per_launch().get(f"fine_step_{args.stack}_mixed")
+    result = {
+        "metric": METRIC,
+        "value": round(value, 4),
+        "unit": "guarded solves/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(ms_mixed / K, 3),
+        "s_per_solve": round(ms_mixed / K / 1e3, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 V-cycle (bf16-stored coarse stencils), f64 FGMRES/Cholesky/guard",
+        "data": "synthetic (seeded void p in {0.2,0.35,0.5}, cone filter r=1.5, SIMP p=3)",
+        "config": {
+            "workload": "guarded SIMP-floor solve, cantilever 160x80x40 (512,000 elements, "
+                        f"{n_free} free DOFs), floors 1e-12|1e-3,1e-2, 4-level GMG ({args.stack} stack), "
+                        "FGMRES restart 300 tol 1e-6, r50/r100 probe 100 its",
+            "global_batch": n_states,
+            "parallelism": f"replicas x{world} (independent states per rank)",
+            "l2": "working set larger than L2 (FGMRES basis + hierarchy > 126 MB); no flush",
+        },
+        "clocks": clk.summary(),
+        "fp64": {
+            "value": round(n_states / (ms_fp64 / 1e3), 4),
+            "unit": "guarded solves/s",
+            "s_per_solve": round(ms_fp64 / K / 1e3, 5),
+            "speedup_mixed_over_fp64": round(ms_fp64 / ms_mixed, 3),
+        },
+        "solves": [
+            {"seed": s, "trigger": r["trigger"], "rho_min": r["recommended_rho_min"],
+             "converged": r["solve_converged"], "iters": r["total_iters"],
+             "true_residual": r["solve_final_rel_residual"], "fp64_iters": f["total_iters"],
+             "fp64_true_residual": f["solve_final_rel_residual"]}
+            for s, r, f in zip(timed_seeds, rows_mixed, rows_fp64)
+        ],
+        "all_guarded": all(r["solve_converged"] for r in rows_mixed + rows_e2e + rows_fp64),
+        "e2e": {
+            "value": round(e2e_value, 4),
+            "unit": "guarded solves/s",
+            "h2d_bytes_per_step": 8 * ne,
+            "d2h_bytes_per_step": 8 * n_free,
+        },
+        "gpu_launches": int(launches),
+        "roofline": {
+            "kernel": f"fine_sweep_kernel<float, {'JAC' if args.stack == 'plain' else 'CHEB'}> (fused smoothing step)",
+            "bound": "hbm",
+            "achieved": round(achieved, 1),
+            "peak": hbm_peak,
+            "peak_kind": peak_kind,
+            "unit": "GB/s",
+            "frac": round(achieved / hbm_peak, 4),
+            "traffic": traffic,
+            "algorithmic_bytes_per_launch": alg_bytes,
+            "avg_launch_us": round(avg.value * 1e3, 3),
+        },
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(states[timed_seeds[0]], rows_fp64[0])
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(density, fp64_row) -> dict:
+    """The oracle (the reference's FP64 method on numpy/scipy) on a bounded sample of
+    one state: one hierarchy setup plus two outer FGMRES iterations, scaled to a
+    full guarded solve with the setup and outer-iteration counts the identical FP64
+    algorithm needed on the GPU for the same state."""
+    from oracle.gmg import GMG
+    from oracle.solver import Operator, cantilever_bc, fgmres
+
+    cores = len(os.sched_getaffinity(0))
+    free, F = cantilever_bc(NX, NY, NZ)
+    op = Operator(NX, NY, NZ, free)
+    Ff = F[free]
+    g = GMG(op, n_levels=4, fine_smoother="fp64", smoother_type="jacobi")
+    E = 1e-12 + (1 - 1e-12) * density ** 3
+    t0 = time.perf_counter()
+    g.setup(E)
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    fgmres(lambda v: op.matvec(v, E), Ff, g.apply, tol=1e-6, maxiter=2, restart=300)
+    t_two = time.perf_counter() - t0
+    iters, setups = int(fp64_row["total_iters"]), int(fp64_row["n_setups"])
+    t_solve = setups * t_setup + iters * (t_two / 2.0)
+    return {"value": round(1.0 / t_solve, 6), "unit": "guarded solves/s", "cores": cores, "kind": "port",
+            "sample": f"oracle setup ({t_setup:.1f} s) + 2 FGMRES iterations ({t_two:.1f} s) on one 512k state, "
+                      f"scaled to {setups} setups + {iters} iterations",
+            "s_per_solve": round(t_solve, 2)}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.gmg import GMG
+    from oracle.policy import run_state
+    from oracle.solver import Operator, cantilever_bc
+
+    H = _filter()
+    free, F = cantilever_bc(NX, NY, NZ)
+    op = Operator(NX, NY, NZ, free)
+    Ff = F[free]
+    g = GMG(op, n_levels=4, fine_smoother="fp64", smoother_type="jacobi")
+    steps = max(1, min(args.steps, 2))
+    times = []
+    for i in range(steps):
+        d = make_state(H, args.warmup + i)
+        t0 = time.perf_counter()
+        run_state(op, g, Ff, lambda rm, d=d: d, penal=3.0, raised=(1e-3, 1e-2), restart=300, maxiter=300)
+        times.append(time.perf_counter() - t0)
+    v = steps / sum(times)
+    cores = len(os.sched_getaffinity(0))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "guarded solves/s", "n_gpus": world,
+        "steps": steps, "warmup": 0, "ms_per_step": round(1e3 * sum(times) / steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "guarded SIMP-floor solve, cantilever 160x80x40 (512,000 elements), damped-Jacobi "
+                               "4-level GMG, FGMRES restart 300 tol 1e-6, floors 1e-12|1e-3,1e-2"},
+        "cpu_baseline": {"value": round(v, 6), "unit": "guarded solves/s", "cores": cores, "kind": "port",
+                         "sample": f"{steps} complete guarded solves (oracle, numpy/scipy FP64)"},
+        "e2e": {"value": round(v, 6), "unit": "guarded solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+if __name__ == "__main__":
+    a = _args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_native(a)

@@ -58,7 +58,7 @@ class GuardedFloorPolicy:
                  high_residual_threshold: float = 1e-2, plateau_residual_threshold: float = 1e-4,
                  plateau_ratio_threshold: float = 0.6, severity_jump_r50_threshold: float = 0.0,
                  severity_jump_rho_min: float = 1e-2, stack: Optional[dict] = None, n_levels: int = 4,
-                 cycle_precision: str = "fp64"):
+                 cycle_precision: str = "fp64", reuse_probe: bool = True):
         flags = dict(CANONICAL_STACK if stack is None else stack)
         (self.spec, self.bc, self.free, self.free_gpu, self.edof_gpu, self.F_free_gpu, self.mf_op,
          self.gmg) = _build_components(preset, n_levels=n_levels, cycle_precision=cycle_precision, **flags)
@@ -77,6 +77,7 @@ class GuardedFloorPolicy:
         self.severity_jump_r50_threshold = float(severity_jump_r50_threshold)
         self.severity_jump_rho_min = float(severity_jump_rho_min)
         self.b_norm = float(torch.linalg.norm(self.F_free_gpu))
+        self.reuse_probe = bool(reuse_probe)
         self.last_x = None
 
     # ---------------------------------------------------------------- moduli
@@ -129,14 +130,22 @@ class GuardedFloorPolicy:
             ladder = self.raised_rho_mins if raise_floor else [self.baseline_rho_min]
         attempts: list[FloorAttempt] = []
         attempted: list[float] = []
-        state = {"selected": None}
+        state = {"selected": None, "reused_probe": False}
+        probe_x = self.last_x
 
         def run_sequence(seq):
             for rho_min in seq:
                 if rho_min in attempted:
                     continue
                 attempted.append(rho_min)
-                a = self.solve_at_floor(density, rho_min, maxiter=self.maxiter, history=[], binary=binary)
+                if self.reuse_probe and rho_min == probe.rho_min and probe.solver_reported_converged:
+                    # The probe stopped on the tolerance before its iteration cap, so the
+                    # driver's repeat solve at this floor (same E, same hierarchy, larger
+                    # cap) is the identical deterministic computation: reuse its result.
+                    a = probe
+                    state["reused_probe"] = True
+                else:
+                    a = self.solve_at_floor(density, rho_min, maxiter=self.maxiter, history=[], binary=binary)
                 attempts.append(a)
                 state["selected"] = a
                 if a.true_converged:
@@ -149,6 +158,8 @@ class GuardedFloorPolicy:
             fallback = True
             run_sequence(self.raised_rho_mins)
             sel = state["selected"]
+        if state["reused_probe"] and sel is probe:
+            self.last_x = probe_x
         failed = [a for a in attempts if a is not sel]
         return {
             "probe_r50": r50,
@@ -174,7 +185,10 @@ class GuardedFloorPolicy:
             "failed_ladder_setup_time_s": sum(a.setup_time_s for a in failed),
             "failed_ladder_solve_time_s": sum(a.solve_time_s for a in failed),
             "recorded_policy_time_s": probe.setup_time_s + probe.solve_time_s
-            + sum(a.setup_time_s + a.solve_time_s for a in attempts),
+            + sum(a.setup_time_s + a.solve_time_s for a in attempts if a is not probe),
+            "selected_reused_probe": int(state["reused_probe"]),
+            "n_setups": 1 + sum(1 for a in attempts if a is not probe),
+            "total_iters": probe.iters + sum(a.iters for a in attempts if a is not probe),
             "probe_history": probe_history,
             "attempts": attempts,
         }

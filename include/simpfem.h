@@ -81,6 +81,21 @@ int simpfem_element_energy(simpfem_mesh* m, const double* u_free, double* ce, vo
  * guard, experiments/phase5/run_gmg_floor_detector_prospective.py:246-247). */
 int simpfem_true_residual(simpfem_mesh* m, const double* E, const double* b_free,
                           const double* x_free, double* out_host, void* stream);
+/* The same guard for callers that must not allocate device memory (no counterpart
+ * in the reference).  A host framework that owns all device memory through its own
+ * pool may forbid a library's cudaMalloc/cudaFree (allocations escape its accounting,
+ * cudaFree synchronises the device); simpfem_true_residual sizes work buffers in the
+ * mesh handle on first use, this entry point allocates nothing.  Inputs are
+ * full-layout vectors (3 * n_nodes, 0 at constrained DOFs); r_full receives
+ * b - K(E) x; *out_host = ||r|| / ||b||.  The reduction scratch is one fixed array of
+ * about 64 KB compiled into the library and resident on every GPU that loads it; the
+ * mesh may have at most 8,388,608 DOFs (SIMPFEM_EINVAL beyond).  All calls on a
+ * device share that array, so calls that overlap on one GPU race: serialise them.
+ * The first call on a device looks up the array's address with that device current;
+ * make it before any stream capture. */
+int simpfem_true_residual_noalloc(simpfem_mesh* m, const double* E, const double* b_full,
+                                  const double* x_full, double* r_full, double* out_host,
+                                  void* stream);
 
 /* Options of the Galerkin GMG hierarchy: the keyword arguments of
  * GalerkinMatFreeGMG.__init__ (gpu_fem/multigrid_v4.py:546-580).  The caller

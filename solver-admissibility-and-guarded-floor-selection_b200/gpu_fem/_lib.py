@@ -101,6 +101,7 @@ _SIGS = {
     "simpfem_node_block_apply": (_I, [_P, _P, _P, _P, _P]),
     "simpfem_element_energy": (_I, [_P, _P, _P, _P]),
     "simpfem_true_residual": (_I, [_P, _P, _P, _P, _P, _P]),
+    "simpfem_true_residual_noalloc": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "simpfem_gmg_default_opts": (None, [_P]),
     "simpfem_gmg_create": (_I, [_P, _P, ctypes.POINTER(_P)]),
     "simpfem_gmg_destroy": (_I, [_P]),

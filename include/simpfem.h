@@ -184,6 +184,15 @@ int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, dou
                 double tol, int maxiter, double* history_host, int history_cap, int* history_len,
                 int* iters, int* converged, void* stream);
 
+/* Coarsest-level dense factorisation: Linv <- L^{-1}, L the lower Cholesky factor
+ * of the SPD row-major n x n device matrix A (A is destroyed; Linv lower with zero
+ * upper).  Replaces cp.linalg.cholesky and its finiteness check in
+ * GalerkinMatFreeGMG.setup (gpu_fem/multigrid_v4.py:1308-1337); the coarse solve
+ * (gpu_fem/multigrid_v4.py:1916-1917) then multiplies by L^{-1} and L^{-T}.
+ * *info_host: 0 on success, else the 1-based index of the first non-positive or
+ * non-finite pivot, or n + 1 when L^{-1} holds a non-finite entry. */
+int simpfem_dense_cholesky_inverse(int n, double* A, double* Linv, int* info_host, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -434,4 +434,16 @@ int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, dou
   SF_API_END
 }
 
+int simpfem_dense_cholesky_inverse(int n, double* A, double* Linv, int* info_host, void* stream) {
+  SF_API_BEGIN
+  if (n < 0 || (n > 0 && (!A || !Linv)) || !info_host)
+    throw InvalidArg{"simpfem_dense_cholesky_inverse: bad argument"};
+  DevBuf info;
+  info.alloc(sizeof(int));
+  SF_CUDA(dense_chol_inverse(A, n, Linv, info.as<int>(), S(stream)));
+  SF_CUDA(cudaMemcpyAsync(info_host, info.p, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+  SF_CUDA(cudaStreamSynchronize(S(stream)));
+  SF_API_END
+}
+
 }  // extern "C"

@@ -1061,8 +1061,7 @@ static void setup_coarsest(Gmg& G) {
       SF_CUDA(launch_stencil_to_dense(L.g, L.K64.as<double>(), G.c_didx.as<int32_t>(), n, G.Adense.as<double>(),
                                       G.st));
       if (eps > 0) SF_CUDA(launch_add_diag(G.Adense.as<double>(), n, eps, G.st));
-      SF_CUDA(dense_cholesky(G.Adense.as<double>(), n, info, G.st));
-      SF_CUDA(launch_all_finite(G.Adense.as<double>(), (int64_t)n * n, info, G.st));
+      SF_CUDA(dense_chol_inverse(G.Adense.as<double>(), n, G.Linv.as<double>(), info, G.st));
       int h = 0;
       SF_CUDA(cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, G.st));
       SF_CUDA(cudaStreamSynchronize(G.st));
@@ -1087,7 +1086,7 @@ static void setup_coarsest(Gmg& G) {
     }
     if (ok) {
       G.LinvT.alloc(8 * (size_t)n * n);
-      SF_CUDA(dense_inverse_from_chol(G.Adense.as<double>(), n, G.Linv.as<double>(), G.LinvT.as<double>(), G.st));
+      SF_CUDA(launch_transpose(G.Linv.as<double>(), n, G.LinvT.as<double>(), G.st));
       G.coarse_mode = 1;
       return;
     }

@@ -179,9 +179,11 @@ cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloo
                               const double* p, const uint8_t* mask, double* out, const int* guard,
                               cudaStream_t s);
 
-cudaError_t dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s);
-cudaError_t dense_inverse_from_chol(const double* L, int n, double* Linv, double* LinvT,
-                                    cudaStream_t s);
+// Linv <- L^{-1} (lower, zero upper) of the Cholesky factor of the SPD row-major
+// A (destroyed).  *info_dev: 0, or the 1-based index of the first non-positive
+// pivot, or n + 1 when L^{-1} holds a non-finite entry.
+cudaError_t dense_chol_inverse(double* A, int n, double* Linv, int* info_dev, cudaStream_t s);
+cudaError_t launch_transpose(const double* A, int n, double* At, cudaStream_t s);
 cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b,
                                   double* tmp, double* x, const int* guard, cudaStream_t s);
 cudaError_t launch_add_diag(double* A, int n, double eps, cudaStream_t s);

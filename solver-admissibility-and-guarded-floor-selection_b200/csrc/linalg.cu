@@ -420,204 +420,6 @@ cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloo
   return sf_launched(1);
 }
 
-// ----------------------------------------------------------------------------
-// Dense FP64 Cholesky (lower, row-major, right-looking, 32-wide panels) for the
-// coarsest level (gpu_fem/multigrid_v4.py:1302-1339 uses cp.linalg.cholesky).
-constexpr int NB = 32;
-
-__global__ void potrf_diag_kernel(double* A, int n, int k0, int* info) {
-  __shared__ double T[NB][NB + 1];
-  const int kb = min(NB, n - k0);
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    T[r][c] = (r < kb && c < kb) ? A[(int64_t)(k0 + r) * n + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  for (int j = 0; j < kb; ++j) {
-    if (threadIdx.x == 0) {
-      const double d = T[j][j];
-      if (!(d > 0.0) || !isfinite(d)) {
-        if (*info == 0) *info = k0 + j + 1;
-        T[j][j] = 1.0;
-      } else {
-        T[j][j] = sqrt(d);
-      }
-    }
-    __syncthreads();
-    for (int i = j + 1 + threadIdx.x; i < kb; i += blockDim.x) T[i][j] /= T[j][j];
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-      const int i = idx / NB, c = idx % NB;
-      if (i > j && c > j && c <= i && i < kb) T[i][c] -= T[i][j] * T[c][j];
-    }
-    __syncthreads();
-  }
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    if (r < kb && c < kb) A[(int64_t)(k0 + r) * n + k0 + c] = (c <= r) ? T[r][c] : 0.0;
-  }
-}
-
-// rows i >= k0 + kb: A[i, k0:k0+kb] <- A[i, k0:k0+kb] * L_kk^{-T}
-__global__ void trsm_panel_kernel(double* A, int n, int k0) {
-  __shared__ double L[NB][NB + 1];
-  const int kb = min(NB, n - k0);
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    L[r][c] = (r < kb && c < kb) ? A[(int64_t)(k0 + r) * n + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  const int i = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double x[NB];
-  double* row = A + (int64_t)i * n + k0;
-  for (int j = 0; j < kb; ++j) {
-    double a = row[j];
-    for (int p = 0; p < j; ++p) a -= x[p] * L[j][p];
-    x[j] = a / L[j][j];
-  }
-  for (int j = 0; j < kb; ++j) row[j] = x[j];
-}
-
-// trailing update A[i][j] -= sum_p A[i][k0+p] * A[j][k0+p], lower tiles only
-__global__ void syrk_update_kernel(double* A, int n, int k0) {
-  const int kb = min(NB, n - k0);
-  const int start = k0 + kb;
-  const int ti = blockIdx.y, tj = blockIdx.x;
-  if (tj > ti) return;
-  const int i0 = start + ti * NB, j0 = start + tj * NB;
-  __shared__ double Pi[NB][NB + 1], Pj[NB][NB + 1];
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    Pi[r][c] = (i0 + r < n && c < kb) ? A[(int64_t)(i0 + r) * n + k0 + c] : 0.0;
-    Pj[r][c] = (j0 + r < n && c < kb) ? A[(int64_t)(j0 + r) * n + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    const int i = i0 + r, j = j0 + c;
-    if (i >= n || j >= n || j > i) continue;
-    double s = 0.0;
-#pragma unroll 8
-    for (int p = 0; p < NB; ++p) s += Pi[r][p] * Pj[c][p];
-    A[(int64_t)i * n + j] -= s;
-  }
-}
-
-cudaError_t dense_cholesky(double* A, int n, int* info_dev, cudaStream_t s) {
-  cudaMemsetAsync(info_dev, 0, sizeof(int), s);
-  for (int k0 = 0; k0 < n; k0 += NB) {
-    potrf_diag_kernel<<<1, 256, 0, s>>>(A, n, k0, info_dev);
-    sf_launched(1);
-    const int kb = std::min(NB, n - k0);
-    const int rest = n - k0 - kb;
-    if (rest > 0) {
-      trsm_panel_kernel<<<div_up(rest, 128), 128, 0, s>>>(A, n, k0);
-      const int nt = div_up(rest, NB);
-      syrk_update_kernel<<<dim3(nt, nt), 256, 0, s>>>(A, n, k0);
-      sf_launched(2);
-    }
-  }
-  return cudaGetLastError();
-}
-
-// Linv = L^{-1} by 32x32 blocks: diagonal blocks inverted independently, then
-// the off-diagonal blocks one block-diagonal at a time,
-//   Linv_ik = -Linv_ii * sum_{j=k}^{i-1} L_ij Linv_jk   (i - k = d),
-// every block of one block-diagonal in parallel.
-__global__ void diag_block_inverse_kernel(const double* __restrict__ L, int n, double* __restrict__ Li) {
-  __shared__ double T[NB][NB + 1];
-  __shared__ double X[NB][NB + 1];
-  const int k0 = blockIdx.x * NB;
-  const int kb = min(NB, n - k0);
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    T[r][c] = (r < kb && c < kb) ? L[(int64_t)(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
-  }
-  __syncthreads();
-  // column c of X solves T x = e_c by forward substitution, one thread per column
-  if (threadIdx.x < NB) {
-    const int c = threadIdx.x;
-    for (int r = 0; r < NB; ++r) {
-      double a = (r == c) ? 1.0 : 0.0;
-      for (int p = c; p < r; ++p) a -= T[r][p] * X[p][c];
-      X[r][c] = (r < c) ? 0.0 : a / T[r][r];
-    }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    if (r < kb && c < kb) Li[(int64_t)(k0 + r) * n + k0 + c] = X[r][c];
-  }
-}
-
-__global__ void offdiag_inverse_kernel(const double* __restrict__ L, int n, int d, double* __restrict__ Li) {
-  const int k = blockIdx.x;
-  const int i = k + d;
-  const int i0 = i * NB, k0 = k * NB;
-  const int ib = min(NB, n - i0), kb = min(NB, n - k0);
-  __shared__ double A[NB][NB + 1], B[NB][NB + 1];
-  const int tr = threadIdx.x / NB;  // 0..7 (256 threads)
-  const int tc = threadIdx.x % NB;
-  double acc[4] = {0, 0, 0, 0};
-  for (int j = k; j < i; ++j) {
-    const int j0 = j * NB;
-    const int jb = min(NB, n - j0);
-    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-      const int r = idx / NB, c = idx % NB;
-      A[r][c] = (r < ib && c < jb) ? L[(int64_t)(i0 + r) * n + j0 + c] : 0.0;
-      B[r][c] = (r < jb && c < kb) ? Li[(int64_t)(j0 + r) * n + k0 + c] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int r = tr + 8 * q;
-#pragma unroll 8
-      for (int p = 0; p < NB; ++p) acc[q] += A[r][p] * B[p][tc];
-    }
-    __syncthreads();
-  }
-  // Li_ik = -Li_ii * acc
-  for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx / NB, c = idx % NB;
-    A[r][c] = (r < ib && c < ib) ? Li[(int64_t)(i0 + r) * n + i0 + c] : 0.0;
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) B[tr + 8 * q][tc] = acc[q];
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int r = tr + 8 * q;
-    double s = 0.0;
-    for (int p = 0; p <= r; ++p) s += A[r][p] * B[p][tc];
-    if (r < ib && tc < kb) Li[(int64_t)(i0 + r) * n + k0 + tc] = -s;
-  }
-}
-
-__global__ void transpose_kernel(const double* __restrict__ A, int n, double* __restrict__ At) {
-  __shared__ double T[32][33];
-  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int i = by + r, j = bx + threadIdx.x;
-    T[r][threadIdx.x] = (i < n && j < n) ? A[(int64_t)i * n + j] : 0.0;
-  }
-  __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int i = bx + r, j = by + threadIdx.x;
-    if (i < n && j < n) At[(int64_t)i * n + j] = T[threadIdx.x][r];
-  }
-}
-
-// Linv (lower) and LinvT (its transpose, upper) from the Cholesky factor L.
-cudaError_t dense_inverse_from_chol(const double* L, int n, double* Linv, double* LinvT, cudaStream_t s) {
-  cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, s);
-  const int nb = div_up(n, NB);
-  diag_block_inverse_kernel<<<nb, 64, 0, s>>>(L, n, Linv);
-  for (int d = 1; d < nb; ++d) offdiag_inverse_kernel<<<nb - d, 256, 0, s>>>(L, n, d, Linv);
-  transpose_kernel<<<dim3(nb, nb), dim3(32, 8), 0, s>>>(Linv, n, LinvT);
-  return sf_launched(nb + 1);
-}
-
 // y = M b over the triangle of a dense row-major M (lower: j <= i, upper: j >= i),
 // one warp per row.
 template <int UPPER>

@@ -112,6 +112,7 @@ _SIGS = {
     "simpfem_gmg_fine_E": (_I, [_P, _P]),
     "simpfem_fgmres": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _P]),
     "simpfem_pcg": (_I, [_P, _P, _P, _P, _D, _I, _P, _I, _P, _P, _P, _P]),
+    "simpfem_dense_cholesky_inverse": (_I, [_I, _P, _P, _P, _P]),
 }
 
 

@@ -79,6 +79,57 @@ __device__ __forceinline__ void epilogue(const EpiArgs& ea, int64_t dof, bool fr
   }
 }
 
+// The same per-DOF epilogues for the three DOFs of one node, with the operands
+// read into registers by load() ahead of the element arithmetic so their
+// latency overlaps it; apply() then evaluates exactly epilogue()'s expressions.
+template <typename T, int EPI>
+struct EpiOperands {
+  bool fr[3];
+  T b[3], di[3], dd[3];
+  __device__ __forceinline__ void load(const EpiArgs& ea, int64_t dof0, const uint8_t* __restrict__ mask) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      fr[c] = mask[dof0 + c] != 0;
+      if (EPI != EPI_APPLY) b[c] = ((const T*)ea.b)[dof0 + c];
+      if (EPI == EPI_CHEB1 || EPI == EPI_CHEB || EPI == EPI_JAC) di[c] = ((const T*)ea.dinv)[dof0 + c];
+      if (EPI == EPI_CHEB) dd[c] = ((const T*)ea.d)[dof0 + c];
+    }
+  }
+  __device__ __forceinline__ void apply(const EpiArgs& ea, int64_t dof, int c, T ku, T x) const {
+    if (EPI == EPI_APPLY) {
+      ((T*)ea.y)[dof] = fr[c] ? ku : T(0);
+    } else if (EPI == EPI_RESID) {
+      ((T*)ea.y)[dof] = fr[c] ? sub_rn(b[c], ku) : T(0);
+    } else if (EPI == EPI_CHEB1) {
+      if (fr[c]) {
+        const T z = mul_rn(di[c], sub_rn(b[c], ku));
+        ((T*)ea.d)[dof] = z;
+        ((T*)ea.xo)[dof] = add_rn(x, mul_rn((T)ea.s1, z));
+      } else {
+        ((T*)ea.d)[dof] = T(0);
+        ((T*)ea.xo)[dof] = T(0);
+      }
+    } else if (EPI == EPI_CHEB) {
+      if (fr[c]) {
+        const T z = mul_rn(di[c], sub_rn(b[c], ku));
+        const T dn = mul_rn((T)ea.s1, add_rn(z, mul_rn((T)ea.s2, dd[c])));
+        ((T*)ea.d)[dof] = dn;
+        ((T*)ea.xo)[dof] = add_rn(x, dn);
+      } else {
+        ((T*)ea.d)[dof] = T(0);
+        ((T*)ea.xo)[dof] = T(0);
+      }
+    } else if (EPI == EPI_JAC) {
+      if (fr[c]) {
+        const T w = mul_rn((T)ea.s1, di[c]);
+        ((T*)ea.xo)[dof] = add_rn(x, mul_rn(w, sub_rn(b[c], ku)));
+      } else {
+        ((T*)ea.xo)[dof] = T(0);
+      }
+    }
+  }
+};
+
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 }  // namespace simpfem

@@ -26,6 +26,7 @@ namespace simpfem {
 
 __constant__ double c_wht64[8][9];
 __constant__ float c_wht32[8][9];
+__constant__ float2 c_wht32x2[8][9];  // c_wht32 duplicated into both lanes of a pair
 __constant__ float c_keb16[576];   // KE rounded to bf16 (stored as float), corner-major order
 __constant__ double c_kediag[24];  // KE diagonal, corner-major order
 __constant__ double c_kenb[8][9];  // 3x3 node-diagonal blocks of KE per corner
@@ -55,6 +56,10 @@ void set_fine_constants(const double* ke576, const WhtBlocks& wb) {
     for (int i = 0; i < 9; ++i) w32[b][i] = (float)wb.b[b][i];
   cudaMemcpyToSymbol(c_wht64, wb.b, sizeof(wb.b));
   cudaMemcpyToSymbol(c_wht32, w32, sizeof(w32));
+  float2 w32x2[8][9];
+  for (int b = 0; b < 8; ++b)
+    for (int i = 0; i < 9; ++i) w32x2[b][i] = make_float2(w32[b][i], w32[b][i]);
+  cudaMemcpyToSymbol(c_wht32x2, w32x2, sizeof(w32x2));
   cudaMemcpyToSymbol(c_keb16, keb, sizeof(keb));
   cudaMemcpyToSymbol(c_kediag, kd, sizeof(kd));
   cudaMemcpyToSymbol(c_kenb, nb, sizeof(nb));
@@ -125,25 +130,12 @@ __device__ __forceinline__ void elem_bf16(const float (&u)[8][3], float E, float
   }
 }
 
-template <typename T>
-__device__ __forceinline__ void load_face(T (&uu)[4][3], const T* __restrict__ u, const Grid& g,
-                                          int p, int je, int ke, bool colv) {
-#pragma unroll
-  for (int q2 = 0; q2 < 4; ++q2) {
-    const int dj = q2 >> 1, dk = q2 & 1;
-    const int j = je + dj, k = ke + dk;
-    const bool ok = p >= 0 && p <= g.nx && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz &&
-                    (colv || q2 == 0);
-    if (ok) {
-      const int64_t node = ((int64_t)p * (g.ny + 1) + j) * (g.nz + 1) + k;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) uu[q2][c] = u[3 * node + c];
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) uu[q2][c] = T(0);
-    }
-  }
-}
+// Each block stages its (bj+1) x (bk+1) node tile of one x-plane in shared
+// memory: a tile row is 3 (bk+1) consecutive values of u, so the block reads it
+// with coalesced loads, one value per thread and row (no node is read four
+// times).  Thread t loads the values t, t + NT, ... of the flattened tile; the
+// offsets do not depend on the plane and are computed once.
+constexpr int kTileLoads = 6;  // enough for every shape with bj >= 2, bk >= 3; launch checks
 
 template <typename T, int EPI, int KMODE, int MAXT>
 __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh, const T* __restrict__ E,
@@ -151,45 +143,109 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
                                                           const T* __restrict__ u, EpiArgs ea) {
   if (guard_off(ea.guard)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* S = reinterpret_cast<T*>(smem_raw);
   const int NT = sh.bj * sh.bk;
+  const int W = 3 * (sh.bk + 1);   // values per tile row
+  const int PV = (sh.bj + 1) * W;  // values per plane tile
+  T* F = reinterpret_cast<T*>(smem_raw);  // face sums [2][12][NT]
+  T* P = F + 24 * NT;                     // node-plane tiles [3][PV]
   const int t = threadIdx.x;
   const int tj = t / sh.bk, tk = t - tj * sh.bk;
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);  // ceil((nz+1)/(bk-1))
   const int bjI = blockIdx.x / nbk, bkI = blockIdx.x - bjI * nbk;
-  const int je = bjI * (sh.bj - 1) - 1 + tj;
-  const int ke = bkI * (sh.bk - 1) - 1 + tk;
+  const int jb = bjI * (sh.bj - 1) - 1;  // first tile node row = first element row (a halo)
+  const int kb = bkI * (sh.bk - 1) - 1;
+  const int je = jb + tj, ke = kb + tk;
   const int i0 = blockIdx.y * sh.cx;
   const int i1 = min(i0 + sh.cx, g.nx + 1);
   const bool colv = je >= 0 && je < g.ny && ke >= 0 && ke < g.nz;
   const bool own = tj >= 1 && tk >= 1 && je <= g.ny && ke <= g.nz;
+  const int64_t NZ1 = g.nz + 1;
+  const int64_t plane_vals = 3 * (int64_t)(g.ny + 1) * NZ1;
 
-  T ulo[4][3], uhi[4][3], carry[4][3];
-  load_face<T>(ulo, u, g, i0 - 1, je, ke, colv);
+  int rel[kTileLoads];
+  bool okq[kTileLoads];
+#pragma unroll
+  for (int q = 0; q < kTileLoads; ++q) {
+    const int v = t + q * NT;
+    const int row = v / W, col = v - row * W;
+    const int j = jb + row, k = kb + col / 3;
+    okq[q] = v < PV && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
+    rel[q] = okq[q] ? (int)(3 * ((int64_t)j * NZ1 + kb) + col) : 0;
+  }
+  auto load_plane = [&](int p, T (&r)[kTileLoads]) {
+    const bool pv = p >= 0 && p <= g.nx;
+    const int64_t base = pv ? (int64_t)p * plane_vals : 0;
+#pragma unroll
+    for (int q = 0; q < kTileLoads; ++q)
+      if (q * NT < PV) r[q] = (pv && okq[q]) ? u[base + rel[q]] : T(0);
+  };
+  auto store_plane = [&](int buf, const T (&r)[kTileLoads]) {
+    T* dst = P + buf * PV;
+#pragma unroll
+    for (int q = 0; q < kTileLoads; ++q) {
+      const int v = t + q * NT;
+      if (q * NT < PV && v < PV) dst[v] = r[q];
+    }
+  };
+  auto read_face = [&](int buf, T (&uu)[4][3]) {
+    const T* src = P + buf * PV;
+#pragma unroll
+    for (int q2 = 0; q2 < 4; ++q2) {
+      const int idx = (tj + (q2 >> 1)) * W + (tk + (q2 & 1)) * 3;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) uu[q2][c] = src[idx + c];
+    }
+  };
+  auto e_index = [&](int ie) { return ((int64_t)ie * g.ny + je) * g.nz + ke; };
+
+  // prologue: planes i0-1 and i0 into the tile buffers, plane i0+1 in flight
+  T pre[kTileLoads];
+  load_plane(i0 - 1, pre);
+  store_plane((i0 + 2) % 3, pre);
+  load_plane(i0, pre);
+  store_plane(i0 % 3, pre);
+  if (i0 + 1 <= i1) load_plane(i0 + 1, pre);
+  T Enext = (colv && i0 - 1 >= 0 && i0 - 1 < g.nx) ? E[e_index(i0 - 1)] : T(0);
+  T carry[4][3];
 #pragma unroll
   for (int q2 = 0; q2 < 4; ++q2)
 #pragma unroll
     for (int c = 0; c < 3; ++c) carry[q2][c] = T(0);
+  __syncthreads();
 
+  // Element plane ie couples node planes ie and ie + 1, both read from the
+  // three rotating tile buffers (plane q in buffer q mod 3).  One barrier per
+  // plane: the tile of plane ie + 2 is written before it and first read after
+  // it, the buffer it overwrites (plane ie - 1) was last read before the
+  // previous barrier, and the face sums alternate between two buffers.
   for (int ie = i0 - 1; ie < i1; ++ie) {
-    load_face<T>(uhi, u, g, ie + 1, je, ke, colv);
-    const bool ev = colv && ie >= 0 && ie < g.nx;
+    if (ie + 2 <= i1) store_plane((ie + 2) % 3, pre);
+    if (ie + 3 <= i1) load_plane(ie + 3, pre);
+    const T Ee = Enext;
+    Enext = (colv && ie + 1 < g.nx) ? E[e_index(ie + 1)] : T(0);
+    const bool do_epi = own && ie >= i0;
+    int64_t node = 0;
+    if (do_epi) node = ((int64_t)ie * (g.ny + 1) + je) * NZ1 + ke;
+    EpiOperands<T, EPI> eo;
+    if (do_epi) eo.load(ea, 3 * node, mask);
+    const int blo = (ie + 3) % 3, bhi = (ie + 1) % 3;
+    // the node's own value, read before the barrier: after it the next
+    // iteration may overwrite this plane's buffer
+    T xv[3];
+    if (do_epi) {
+      const T* xs = P + blo * PV + tj * W + tk * 3;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xv[c] = xs[c];
+    }
     T f[8][3];
-    if (ev) {
+    if (colv && ie >= 0 && ie < g.nx) {
       T ue[8][3];
-#pragma unroll
-      for (int q2 = 0; q2 < 4; ++q2)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          ue[q2][c] = ulo[q2][c];
-          ue[4 + q2][c] = uhi[q2][c];
-        }
-      const T Ee = E[((int64_t)ie * g.ny + je) * g.nz + ke];
+      read_face(blo, reinterpret_cast<T(&)[4][3]>(ue[0]));
+      read_face(bhi, reinterpret_cast<T(&)[4][3]>(ue[4]));
       if (KMODE == 0) {
         elem_wht<T>(ue, Ee, f);
       } else {
-        elem_bf16(reinterpret_cast<const float(&)[8][3]>(ue), (float)Ee,
-                  reinterpret_cast<float(&)[8][3]>(f));
+        elem_bf16(reinterpret_cast<const float(&)[8][3]>(ue), (float)Ee, reinterpret_cast<float(&)[8][3]>(f));
       }
     } else {
 #pragma unroll
@@ -197,33 +253,35 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
 #pragma unroll
         for (int c = 0; c < 3; ++c) f[q][c] = T(0);
     }
+    T* buf = F + (ie & 1) * 12 * NT;
     if (ie >= i0) {
-      T* buf = S + ((ie - i0) & 1) * 12 * NT;
 #pragma unroll
       for (int q2 = 0; q2 < 4; ++q2)
 #pragma unroll
         for (int c = 0; c < 3; ++c) buf[(q2 * 3 + c) * NT + t] = carry[q2][c] + f[q2][c];
-      __syncthreads();
-      if (own) {
-        const int64_t node = ((int64_t)ie * (g.ny + 1) + je) * (g.nz + 1) + ke;
+    }
+    __syncthreads();
+    if (do_epi) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T ku = ((buf[(0 * 3 + c) * NT + t] + buf[(2 * 3 + c) * NT + t - sh.bk]) +
-                        buf[(1 * 3 + c) * NT + t - 1]) +
-                       buf[(3 * 3 + c) * NT + t - sh.bk - 1];
-          const int64_t dof = 3 * node + c;
-          epilogue<T, EPI>(ea, dof, mask[dof] != 0, ku, ulo[0][c]);
-        }
+      for (int c = 0; c < 3; ++c) {
+        const T ku = ((buf[(0 * 3 + c) * NT + t] + buf[(2 * 3 + c) * NT + t - sh.bk]) +
+                      buf[(1 * 3 + c) * NT + t - 1]) +
+                     buf[(3 * 3 + c) * NT + t - sh.bk - 1];
+        eo.apply(ea, 3 * node + c, c, ku, xv[c]);
       }
     }
 #pragma unroll
     for (int q2 = 0; q2 < 4; ++q2)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        carry[q2][c] = f[4 + q2][c];
-        ulo[q2][c] = uhi[q2][c];
-      }
+      for (int c = 0; c < 3; ++c) carry[q2][c] = f[4 + q2][c];
   }
+}
+
+template <typename T>
+static size_t sweep_smem(const SweepShape& sh) {
+  const size_t NT = (size_t)sh.bj * sh.bk;
+  const size_t PV = (size_t)(sh.bj + 1) * 3 * (sh.bk + 1);
+  return (24 * NT + 3 * PV) * sizeof(T);
 }
 
 template <typename T, int EPI, int KMODE, int MAXT>
@@ -231,7 +289,8 @@ static cudaError_t launch_sweep(const Grid& g, const SweepShape& sh, const T* E,
                                 const T* u, const EpiArgs& ea, cudaStream_t s) {
   const int NT = sh.bj * sh.bk;
   if (NT > MAXT || sh.bj < 2 || sh.bk < 2 || sh.cx < 1) return cudaErrorInvalidConfiguration;
-  const size_t smem = (size_t)2 * 12 * NT * sizeof(T);
+  if ((int64_t)(sh.bj + 1) * 3 * (sh.bk + 1) > (int64_t)kTileLoads * NT) return cudaErrorInvalidConfiguration;
+  const size_t smem = sweep_smem<T>(sh);
   static bool attr_done = false;
   if (!attr_done) {
     cudaFuncSetAttribute(fine_sweep_kernel<T, EPI, KMODE, MAXT>,
@@ -242,6 +301,235 @@ static cudaError_t launch_sweep(const Grid& g, const SweepShape& sh, const T* E,
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
   dim3 grid(nbj * nbk, div_up(g.nx + 1, sh.cx));
   fine_sweep_kernel<T, EPI, KMODE, MAXT><<<grid, NT, smem, s>>>(g, sh, E, mask, u, ea);
+  return sf_launched(1);
+}
+
+// ----------------------------------------------------------------------------
+// FP32 sweep with two elements per thread.  Thread (tj, tp) evaluates the
+// k-adjacent element columns tk = 2tp and 2tp + 1 of the block's tile with the
+// packed FP32 pair instructions of sm_100 (lane x: element 2tp, lane y: element
+// 2tp + 1), which halves the arithmetic instruction count; it owns the nodes at
+// those two positions.  The node tile is stored component-major in shared
+// memory ([c][row][k], rows padded to an even length) so the dk = 0 corner pair
+// of both elements is one aligned 64-bit load.  Elements outside the mesh get
+// E = 0 (their corner values are zero-filled, so they contribute exactly 0)
+// instead of a branch.  Same staging, barrier and summation order as
+// fine_sweep_kernel; 32-bit indexing (the launcher checks ndof < 2^31).
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);  // a - b, one rounding
+}
+
+__device__ __forceinline__ void wht8x2(float2 (&a)[8]) {
+#pragma unroll
+  for (int m = 4; m >= 1; m >>= 1) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      if ((q & m) == 0) {
+        const float2 p = a[q], r = a[q | m];
+        a[q] = __fadd2_rn(p, r);
+        a[q | m] = f2sub(p, r);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void elem_wht_x2(const float2 (&u)[8][3], float2 E, float2 (&f)[8][3]) {
+  float2 w[3][8];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) w[c][q] = u[q][c];
+    wht8x2(w[c]);
+  }
+  float2 v[3][8];
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const float2 in0 = w[0][b ^ 4], in1 = w[1][b ^ 2], in2 = w[2][b ^ 1];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      float2 s = __fmul2_rn(c_wht32x2[b][3 * r], in0);
+      s = __ffma2_rn(c_wht32x2[b][3 * r + 1], in1, s);
+      s = __ffma2_rn(c_wht32x2[b][3 * r + 2], in2, s);
+      v[r][b ^ (4 >> r)] = __fmul2_rn(E, s);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    wht8x2(v[c]);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) f[q][c] = v[c][q];
+  }
+}
+
+constexpr int kX2Threads = 256;
+constexpr int kX2NodeLoads = 3;  // tile nodes per thread; launch checks
+
+template <int EPI>
+__global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, SweepShape sh,
+                                                                   const float* __restrict__ E,
+                                                                   const uint8_t* __restrict__ mask,
+                                                                   const float* __restrict__ u, EpiArgs ea) {
+  if (guard_off(ea.guard)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int HK = sh.bk >> 1, NT = sh.bj * HK, NE = sh.bj * sh.bk;
+  const int NK1 = sh.bk + 1, NKP = sh.bk + 2;
+  const int RP = (sh.bj + 1) * NKP;  // one component of one plane tile
+  const int PV = 3 * RP;
+  const int NN = (sh.bj + 1) * NK1;  // tile nodes
+  float* F = reinterpret_cast<float*>(smem_raw);  // face sums [2][12][NE]
+  float* P = F + 24 * NE;                         // plane tiles [3][3][bj+1][NKP]
+  const int t = threadIdx.x;
+  const int tj = t / HK, tp = t - tj * HK, tk0 = 2 * tp;
+  const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
+  const int bjI = blockIdx.x / nbk, bkI = blockIdx.x - bjI * nbk;
+  const int jb = bjI * (sh.bj - 1) - 1, kb = bkI * (sh.bk - 1) - 1;
+  const int je = jb + tj, ke0 = kb + tk0, ke1 = ke0 + 1;
+  const int i0 = blockIdx.y * sh.cx;
+  const int i1 = min(i0 + sh.cx, g.nx + 1);
+  const bool rowv = je >= 0 && je < g.ny;
+  const bool colv0 = rowv && ke0 >= 0 && ke0 < g.nz, colv1 = rowv && ke1 >= 0 && ke1 < g.nz;
+  const bool ownr = tj >= 1 && je <= g.ny;
+  const bool own0 = ownr && tk0 >= 1 && ke0 <= g.nz, own1 = ownr && ke1 <= g.nz;
+  const int NZ1 = g.nz + 1;
+  const int64_t plane_vals = 3 * (int64_t)(g.ny + 1) * NZ1;
+
+  int rel[kX2NodeLoads], sidx[kX2NodeLoads];
+  bool okn[kX2NodeLoads];
+#pragma unroll
+  for (int s = 0; s < kX2NodeLoads; ++s) {
+    const int n = t + s * NT;
+    const int row = n / NK1, kk = n - row * NK1;
+    const int j = jb + row, k = kb + kk;
+    okn[s] = n < NN && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
+    rel[s] = okn[s] ? 3 * (j * NZ1 + k) : 0;
+    sidx[s] = n < NN ? row * NKP + kk : -1;
+  }
+  auto load_plane = [&](int p, float (&r)[3 * kX2NodeLoads]) {
+    const bool pv = p >= 0 && p <= g.nx;
+    const float* base = u + (pv ? (int64_t)p * plane_vals : 0);
+#pragma unroll
+    for (int s = 0; s < kX2NodeLoads; ++s)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) r[3 * s + c] = (pv && okn[s]) ? base[rel[s] + c] : 0.f;
+  };
+  auto store_plane = [&](int buf, const float (&r)[3 * kX2NodeLoads]) {
+    float* dst = P + buf * PV;
+#pragma unroll
+    for (int s = 0; s < kX2NodeLoads; ++s)
+      if (sidx[s] >= 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[c * RP + sidx[s]] = r[3 * s + c];
+      }
+  };
+  auto read_face2 = [&](int buf, float2 (&uu)[8][3], int q0) {
+    const float* src = P + buf * PV;
+#pragma unroll
+    for (int q2 = 0; q2 < 4; ++q2) {
+      const int base = (tj + (q2 >> 1)) * NKP + tk0 + (q2 & 1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float* a = src + c * RP + base;
+        uu[q0 + q2][c] = (q2 & 1) ? make_float2(a[0], a[1]) : *reinterpret_cast<const float2*>(a);
+      }
+    }
+  };
+  auto e_pair = [&](int ie) {
+    const bool pv = ie >= 0 && ie < g.nx;
+    const int idx = (ie * g.ny + je) * g.nz + ke0;
+    return make_float2((pv && colv0) ? E[idx] : 0.f, (pv && colv1) ? E[idx + 1] : 0.f);
+  };
+
+  float pre[3 * kX2NodeLoads];
+  load_plane(i0 - 1, pre);
+  store_plane((i0 + 2) % 3, pre);
+  load_plane(i0, pre);
+  store_plane(i0 % 3, pre);
+  if (i0 + 1 <= i1) load_plane(i0 + 1, pre);
+  float2 En = e_pair(i0 - 1);
+  float2 carry[4][3];
+#pragma unroll
+  for (int q2 = 0; q2 < 4; ++q2)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) carry[q2][c] = make_float2(0.f, 0.f);
+  __syncthreads();
+
+  const int e0 = tj * sh.bk + tk0;
+  const int em1 = tp == 0 ? e0 : e0 - 1;  // node 2tp is a halo when tp == 0
+  for (int ie = i0 - 1; ie < i1; ++ie) {
+    if (ie + 2 <= i1) store_plane((ie + 2) % 3, pre);
+    if (ie + 3 <= i1) load_plane(ie + 3, pre);
+    const float2 Ee = En;
+    En = e_pair(ie + 1);
+    const bool epi0 = own0 && ie >= i0, epi1 = own1 && ie >= i0;
+    const int node0 = (ie * (g.ny + 1) + je) * NZ1 + ke0;
+    EpiOperands<float, EPI> eo0, eo1;
+    if (epi0) eo0.load(ea, 3 * (int64_t)node0, mask);
+    if (epi1) eo1.load(ea, 3 * (int64_t)node0 + 3, mask);
+    const int blo = (ie + 3) % 3, bhi = (ie + 1) % 3;
+    float2 xv[3];
+    if (epi0 || epi1) {
+      const float* xs = P + blo * PV + tj * NKP + tk0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xv[c] = *reinterpret_cast<const float2*>(xs + c * RP);
+    }
+    float2 f[8][3];
+    {
+      float2 ue[8][3];
+      read_face2(blo, ue, 0);
+      read_face2(bhi, ue, 4);
+      elem_wht_x2(ue, Ee, f);
+    }
+    float* Fb = F + (ie & 1) * 12 * NE;
+    if (ie >= i0) {
+#pragma unroll
+      for (int q2 = 0; q2 < 4; ++q2)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          *reinterpret_cast<float2*>(Fb + (q2 * 3 + c) * NE + e0) = __fadd2_rn(carry[q2][c], f[q2][c]);
+    }
+    __syncthreads();
+    if (epi0 || epi1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float2 a = *reinterpret_cast<const float2*>(Fb + (0 * 3 + c) * NE + e0);
+        const float2 b = *reinterpret_cast<const float2*>(Fb + (2 * 3 + c) * NE + e0 - sh.bk);
+        const float* p1 = Fb + (1 * 3 + c) * NE;
+        const float* p3 = Fb + (3 * 3 + c) * NE - sh.bk;
+        const float2 x1 = make_float2(p1[em1], p1[e0]);
+        const float2 x3 = make_float2(p3[em1], p3[e0]);
+        const float2 ku = __fadd2_rn(__fadd2_rn(__fadd2_rn(a, b), x1), x3);
+        if (epi0) eo0.apply(ea, 3 * (int64_t)node0 + c, c, ku.x, xv[c].x);
+        if (epi1) eo1.apply(ea, 3 * (int64_t)node0 + 3 + c, c, ku.y, xv[c].y);
+      }
+    }
+#pragma unroll
+    for (int q2 = 0; q2 < 4; ++q2)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) carry[q2][c] = f[4 + q2][c];
+  }
+}
+
+static bool x2_shape_ok(const Grid& g, const SweepShape& sh) {
+  const int NT = sh.bj * sh.bk / 2;
+  return sh.bk % 2 == 0 && sh.bk >= 4 && sh.bj >= 3 && sh.cx >= 1 && NT <= kX2Threads &&
+         (sh.bj + 1) * (sh.bk + 1) <= kX2NodeLoads * NT && g.ndof < (int64_t(1) << 31);
+}
+
+template <int EPI>
+static cudaError_t launch_sweep_f32(const Grid& g, const SweepShape& sh, const float* E, const uint8_t* mask,
+                                    const float* u, const EpiArgs& ea, cudaStream_t s) {
+  if (!x2_shape_ok(g, sh)) return launch_sweep<float, EPI, 0, 512>(g, sh, E, mask, u, ea, s);
+  const int NT = sh.bj * sh.bk / 2, NE = sh.bj * sh.bk;
+  const size_t smem = sizeof(float) * (24 * (size_t)NE + 9 * (size_t)(sh.bj + 1) * (sh.bk + 2));
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = true;
+  }
+  const int nbj = (g.ny + sh.bj - 1) / (sh.bj - 1);
+  const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
+  dim3 grid(nbj * nbk, div_up(g.nx + 1, sh.cx));
+  fine_sweep_x2_kernel<EPI><<<grid, NT, smem, s>>>(g, sh, E, mask, u, ea);
   return sf_launched(1);
 }
 
@@ -263,11 +551,16 @@ cudaError_t launch_fine(DType t, Epi epi, const Grid& g, const SweepShape& sh, c
     }
   } else if (t == F32) {
     switch (epi) {
-      SF_FINE_CASE(float, kMaxThreadsF32, EPI_APPLY)
-      SF_FINE_CASE(float, kMaxThreadsF32, EPI_RESID)
-      SF_FINE_CASE(float, kMaxThreadsF32, EPI_CHEB1)
-      SF_FINE_CASE(float, kMaxThreadsF32, EPI_CHEB)
-      SF_FINE_CASE(float, kMaxThreadsF32, EPI_JAC)
+      case EPI_APPLY:
+        return launch_sweep_f32<EPI_APPLY>(g, sh, (const float*)E, mask, (const float*)u, ea, s);
+      case EPI_RESID:
+        return launch_sweep_f32<EPI_RESID>(g, sh, (const float*)E, mask, (const float*)u, ea, s);
+      case EPI_CHEB1:
+        return launch_sweep_f32<EPI_CHEB1>(g, sh, (const float*)E, mask, (const float*)u, ea, s);
+      case EPI_CHEB:
+        return launch_sweep_f32<EPI_CHEB>(g, sh, (const float*)E, mask, (const float*)u, ea, s);
+      case EPI_JAC:
+        return launch_sweep_f32<EPI_JAC>(g, sh, (const float*)E, mask, (const float*)u, ea, s);
     }
   } else if (t == BF16) {
     // BF16 operands (u and KE rounded to bf16), FP32 accumulation and FP32 vectors.

@@ -376,8 +376,8 @@ __global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, Sweep
   const int RP = (sh.bj + 1) * NKP;  // one component of one plane tile
   const int PV = 3 * RP;
   const int NN = (sh.bj + 1) * NK1;  // tile nodes
-  float* F = reinterpret_cast<float*>(smem_raw);  // face sums [2][12][NE]
-  float* P = F + 24 * NE;                         // plane tiles [3][3][bj+1][NKP]
+  float* F = reinterpret_cast<float*>(smem_raw);  // face sums [3][12][NE], plane q in q mod 3
+  float* P = F + 36 * NE;                         // plane tiles [3][3][bj+1][NKP]
   const int t = threadIdx.x;
   const int tj = t / HK, tp = t - tj * HK, tk0 = 2 * tp;
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
@@ -446,11 +446,6 @@ __global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, Sweep
   store_plane(i0 % 3, pre);
   if (i0 + 1 <= i1) load_plane(i0 + 1, pre);
   float2 En = e_pair(i0 - 1);
-  float2 carry[4][3];
-#pragma unroll
-  for (int q2 = 0; q2 < 4; ++q2)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) carry[q2][c] = make_float2(0.f, 0.f);
   __syncthreads();
 
   const int e0 = tj * sh.bk + tk0;
@@ -462,16 +457,7 @@ __global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, Sweep
     En = e_pair(ie + 1);
     const bool epi0 = own0 && ie >= i0, epi1 = own1 && ie >= i0;
     const int node0 = (ie * (g.ny + 1) + je) * NZ1 + ke0;
-    EpiOperands<float, EPI> eo0, eo1;
-    if (epi0) eo0.load(ea, 3 * (int64_t)node0, mask);
-    if (epi1) eo1.load(ea, 3 * (int64_t)node0 + 3, mask);
     const int blo = (ie + 3) % 3, bhi = (ie + 1) % 3;
-    float2 xv[3];
-    if (epi0 || epi1) {
-      const float* xs = P + blo * PV + tj * NKP + tk0;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) xv[c] = *reinterpret_cast<const float2*>(xs + c * RP);
-    }
     float2 f[8][3];
     {
       float2 ue[8][3];
@@ -479,14 +465,31 @@ __global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, Sweep
       read_face2(bhi, ue, 4);
       elem_wht_x2(ue, Ee, f);
     }
-    float* Fb = F + (ie & 1) * 12 * NE;
-    if (ie >= i0) {
+    // epilogue operands after the element arithmetic (not live across its
+    // register peak); the face-sum stores and the barrier cover their latency
+    EpiOperands<float, EPI> eo0, eo1;
+    if (epi0) eo0.load(ea, 3 * (int64_t)node0, mask);
+    if (epi1) eo1.load(ea, 3 * (int64_t)node0 + 3, mask);
+    float2 xv[3];
+    if (epi0 || epi1) {
+      const float* xs = P + blo * PV + tj * NKP + tk0;
 #pragma unroll
-      for (int q2 = 0; q2 < 4; ++q2)
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          *reinterpret_cast<float2*>(Fb + (q2 * 3 + c) * NE + e0) = __fadd2_rn(carry[q2][c], f[q2][c]);
+      for (int c = 0; c < 3; ++c) xv[c] = *reinterpret_cast<const float2*>(xs + c * RP);
     }
+    // face sums of node plane ie: this element plane's -x face added to the
+    // +x face of element plane ie - 1, which this thread parked in the same
+    // slots one iteration earlier; the +x face goes to plane ie + 1's buffer
+    // (last read before the previous barrier)
+    float* Fb = F + ((ie + 3) % 3) * 12 * NE;
+    float* Fn = F + ((ie + 1) % 3) * 12 * NE;
+#pragma unroll
+    for (int q2 = 0; q2 < 4; ++q2)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2* slot = reinterpret_cast<float2*>(Fb + (q2 * 3 + c) * NE + e0);
+        if (ie >= i0) *slot = __fadd2_rn(*slot, f[q2][c]);
+        *reinterpret_cast<float2*>(Fn + (q2 * 3 + c) * NE + e0) = f[4 + q2][c];
+      }
     __syncthreads();
     if (epi0 || epi1) {
 #pragma unroll
@@ -502,10 +505,6 @@ __global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, Sweep
         if (epi1) eo1.apply(ea, 3 * (int64_t)node0 + 3 + c, c, ku.y, xv[c].y);
       }
     }
-#pragma unroll
-    for (int q2 = 0; q2 < 4; ++q2)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) carry[q2][c] = f[4 + q2][c];
   }
 }
 
@@ -520,7 +519,7 @@ static cudaError_t launch_sweep_f32(const Grid& g, const SweepShape& sh, const f
                                     const float* u, const EpiArgs& ea, cudaStream_t s) {
   if (!x2_shape_ok(g, sh)) return launch_sweep<float, EPI, 0, 512>(g, sh, E, mask, u, ea, s);
   const int NT = sh.bj * sh.bk / 2, NE = sh.bj * sh.bk;
-  const size_t smem = sizeof(float) * (24 * (size_t)NE + 9 * (size_t)(sh.bj + 1) * (sh.bk + 2));
+  const size_t smem = sizeof(float) * (36 * (size_t)NE + 9 * (size_t)(sh.bj + 1) * (sh.bk + 2));
   static bool attr_done = false;
   if (!attr_done) {
     cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -218,6 +218,9 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
   SF_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   SweepShape best_sh = default_shape(m.g, maxt);
+  // SIMPFEM_TUNE_VERBOSE=1 prints every candidate's time (stderr)
+  const char* vb = getenv("SIMPFEM_TUNE_VERBOSE");
+  const bool verbose = vb != nullptr && vb[0] != '\0' && vb[0] != '0';
   EpiArgs ea;
   ea.y = y.p;
   for (const SweepShape& sh : cands) {
@@ -233,6 +236,9 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
     SF_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     SF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (verbose)
+      fprintf(stderr, "[simpfem tune] %s %dx%dx%d bj=%d bk=%d cx=%d: %.1f us\n", t == F64 ? "f64" : "f32", m.g.nx,
+              m.g.ny, m.g.nz, sh.bj, sh.bk, sh.cx, ms * 1000.f / 3.f);
     if (ms < best) {
       best = ms;
       best_sh = sh;

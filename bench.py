@@ -10,7 +10,12 @@ radius 1.5, E = 1e-12 + (1 - 1e-12) rho_f^3, unit tip load, x = 0 face clamped.
 The hierarchy is the damped-Jacobi V-cycle (4 levels, FGMRES restart 300,
 tol 1e-6); ``--stack canonical`` selects the reference drivers' default stack.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
+The mixed arm (``value``, ``e2e``) is the mixed-precision, batched form:
+``--width`` states in flight per GPU (gpu_fem.policy.BatchedFloorPolicy, one
+hierarchy and CUDA stream per worker).  The ``fp64`` object is the plain FP64
+form from scratch, one state at a time, on the same states.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--width B] [--impl native|reference]
 
 N > 1 (torchrun): ranks solve disjoint states, no collective on the data path;
 the reported value is all states / max-over-ranks time.
@@ -44,18 +49,19 @@ METRIC = "guarded solves/s & s/solve to true resid 1e-6 @512k elems: mixed vs FP
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=6)
+    ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--stack", default="plain", choices=["plain", "canonical"])
+    ap.add_argument("--width", type=int, default=4, help="states in flight per GPU in the mixed arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
 def _filter():
-    from oracle.solver import density_filter
+    from gpu_fem.pub_simp_solver import _build_density_filter
 
-    return density_filter(NX, NY, NZ, 1.5)
+    return _build_density_filter(NX, NY, 1.5, NZ)
 
 
 def make_state(H, seed: int) -> np.ndarray:
@@ -140,7 +146,7 @@ def run_native(args):
     import torch.distributed as dist
 
     from gpu_fem import _lib
-    from gpu_fem.policy import GuardedFloorPolicy
+    from gpu_fem.policy import BatchedFloorPolicy, GuardedFloorPolicy
     from gpu_fem.presets import cantilever_spec
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -151,14 +157,18 @@ def run_native(args):
         dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
     H = _filter()
     spec = cantilever_spec(NX, NY, NZ)
-    K, W = args.steps, args.warmup
-    seeds = [1000 * rank + i for i in range(W + 2 * K)]
+    K, W, B = args.steps, args.warmup, max(1, args.width)
+    WB = max(W, B)  # warm-up states for the batched arm: every worker sees at least one
+    seeds = [1000 * rank + i for i in range(WB + 2 * K)]
     states = {s: make_state(H, s) for s in seeds}
 
+    def policy_kwargs(precision):
+        return dict(penal=3.0, tol=1e-6, restart=300, maxiter=300, probe_iters=100, probe_r50=50,
+                    raised_rho_mins=(1e-3, 1e-2), stack=_stack(args.stack, precision),
+                    cycle_precision="fp32" if precision == "mixed" else "fp64")
+
     def policy(precision):
-        return GuardedFloorPolicy(spec, penal=3.0, tol=1e-6, restart=300, maxiter=300, probe_iters=100,
-                                  probe_r50=50, raised_rho_mins=(1e-3, 1e-2), stack=_stack(args.stack, precision),
-                                  cycle_precision="fp32" if precision == "mixed" else "fp64")
+        return GuardedFloorPolicy(spec, **policy_kwargs(precision))
 
     def barrier():
         if world > 1:
@@ -190,14 +200,40 @@ def run_native(args):
             ms = float(t.item())
         return ms, rows, launches
 
-    mixed = policy("mixed")
-    for s in seeds[:W]:
-        mixed.run(torch.as_tensor(states[s], device="cuda"))
-    timed_seeds = seeds[W:W + K]
+    def timed_batch(bp, seq, host_io: bool):
+        # host_io: pinned host densities in, each solution x back to the host, inside the timed region
+        if host_io:
+            dens = [torch.as_tensor(states[s]).pin_memory() for s in seq]
+        else:
+            dens = [torch.as_tensor(states[s], device="cuda") for s in seq]
+        xs = {}
+
+        def keep_x(k, worker, row):
+            xs[k] = worker.last_x.to("cpu")
+
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = _lib.lib().simpfem_launch_count()
+        e0.record()
+        rows = bp.run_many(dens, on_result=keep_x if host_io else None)
+        e1.record()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        launches = _lib.lib().simpfem_launch_count() - l0
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, rows, launches
+
+    # mixed precision, B states in flight (one hierarchy and stream per worker)
+    mixed = BatchedFloorPolicy(B, spec, **policy_kwargs("mixed"))
+    mixed.run_many([torch.as_tensor(states[s], device="cuda") for s in seeds[:WB]])
+    timed_seeds = seeds[WB:WB + K]
     with ClockSampler(local) as clk:
-        ms_mixed, rows_mixed, launches = timed(mixed, timed_seeds, host_io=False)
-    ms_e2e, rows_e2e, _ = timed(mixed, seeds[W + K:W + 2 * K], host_io=True)
-    # FP64 from-scratch comparison on the same states
+        ms_mixed, rows_mixed, launches = timed_batch(mixed, timed_seeds, host_io=False)
+    ms_e2e, rows_e2e, _ = timed_batch(mixed, seeds[WB + K:WB + 2 * K], host_io=True)
+    # plain FP64 from scratch, one state at a time, on the same states
     fp64 = policy("fp64")
     for s in seeds[:W]:
         fp64.run(torch.as_tensor(states[s], device="cuda"))
@@ -206,12 +242,13 @@ def run_native(args):
     n_states = K * world
     value = n_states / (ms_mixed / 1e3)
     e2e_value = n_states / (ms_e2e / 1e3)
-    n_free = int(mixed.F_free_gpu.numel())
+    n_free = int(mixed.workers[0].F_free_gpu.numel())
 
     # roofline of the dominant kernel: the fused fine smoothing step of the cycle
     hbm_peak, peak_kind = _peaks()
     avg = ctypes.c_float()
-    _lib.call("simpfem_gmg_time_smoother_step", mixed.gmg._h, 0, 50, ctypes.byref(avg), _lib.stream_ptr())
+    _lib.call("simpfem_gmg_time_smoother_step", mixed.workers[0].gmg._h, 0, 50, ctypes.byref(avg),
+              _lib.stream_ptr())
     ndof = 3 * (NX + 1) * (NY + 1) * (NZ + 1)
     ne = NX * NY * NZ
     # fp32 vectors read u, rhs, dinv (plus d for Chebyshev) and write x (plus d); E (fp32); 1-byte DOF mask
@@ -238,7 +275,8 @@ def run_native(args):
                         f"{n_free} free DOFs), floors 1e-12|1e-3,1e-2, 4-level GMG ({args.stack} stack), "
                         "FGMRES restart 300 tol 1e-6, r50/r100 probe 100 its",
             "global_batch": n_states,
-            "parallelism": f"replicas x{world} (independent states per rank)",
+            "batch_width": B,
+            "parallelism": f"{B} states in flight per GPU (one stream each) x {world} replicas",
             "l2": "working set larger than L2 (FGMRES basis + hierarchy > 126 MB); no flush",
         },
         "clocks": clk.summary(),

@@ -49,12 +49,16 @@ struct DGemm {
 
 // C = alpha * A op(B) + beta * C on the FP64 tensor cores (mma.sync m8n8k4):
 // 64x64 CTA tiles, 4 warps each owning a 32x32 warp tile (4 x 4 MMA tiles),
-// 16-deep K steps staged through padded shared memory with one
-// register-staged prefetch of the next K step.  A is row-major (A[i*lda + p]);
-//   TB = 0: op(B)[p][j] = B[p*ldb + j];  TB = 1: op(B)[p][j] = B[j*ldb + p].
-// The shared-memory row stride of 68 doubles puts the 16 (k, m) pairs a half
-// warp reads for one fragment in 16 distinct banks.
-constexpr int SST = 68;
+// 16-deep K steps streamed through a 4-stage cp.async pipeline (8-byte copies,
+// zero-filled outside the matrix, so any leading dimension works).  A is
+// row-major (A[i*lda + p]) and kept [m][k] in shared memory;
+//   TB = 0: op(B)[p][j] = B[p*ldb + j], kept [k][n];
+//   TB = 1: op(B)[p][j] = B[j*ldb + p], kept [n][k].
+// Row strides of 20 ([m][k], [n][k]) and 68 ([k][n]) doubles put the 32 values
+// of one fragment read in 16 banks twice each, the minimum of two wavefronts.
+constexpr int KST = 20, NST = 68, NSTAGE = 4;
+constexpr int A_STAGE = GM * KST;                       // doubles per stage
+constexpr int B_STAGE_T = GN * KST, B_STAGE_N = GK * NST;
 
 __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -62,10 +66,22 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
                : "d"(a), "d"(b));
 }
 
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
 template <int TB>
 __global__ void __launch_bounds__(GT) dgemm_kernel(DGemm g) {
-  __shared__ __align__(16) double As[2][GK][SST];
-  __shared__ __align__(16) double Bs[2][GK][SST];
+  extern __shared__ __align__(16) double dsm[];
+  double* As = dsm;                         // [NSTAGE][GM][KST]
+  double* Bs = dsm + NSTAGE * A_STAGE;      // [NSTAGE][GN][KST] or [NSTAGE][GK][NST]
+  constexpr int BSTG = TB ? B_STAGE_T : B_STAGE_N;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int wm = w >> 1, wn = w & 1;
   const int i0 = blockIdx.y * GM, j0 = blockIdx.x * GN;
@@ -74,43 +90,35 @@ __global__ void __launch_bounds__(GT) dgemm_kernel(DGemm g) {
   if (g.tri == TRI_OPA_LOWER) kend = min(kend, i0 + GM);
   if (g.tri == TRI_OPB_UPPER) kend = min(kend, j0 + GN);
   if (g.tri == TRI_OPB_LOWER) kbeg = j0;
-  // loads: "row-run" = one matrix row, 8 consecutive k; "k-run" = one k row,
-  // four pairs of consecutive columns 16 apart
+  const int nk = kend > kbeg ? (kend - kbeg + GK - 1) / GK : 0;
+  // copy mappings: "row-run" = one matrix row, 8 consecutive k; "k-run" = one
+  // k row, 8 consecutive columns
   const int ar = t >> 1, ak = (t & 1) * 8;
-  const int bkr = t >> 3, bj = (t & 7) * 2;
-  double ra[8], rb[8];
-  auto gload = [&](int k0) {
+  const int bkr = t >> 3, bj = (t & 7) * 8;
+
+  auto issue = [&](int stage, int k0) {
+    double* as = As + stage * A_STAGE;
+    double* bs = Bs + stage * BSTG;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int i = i0 + ar, p = k0 + ak + q;
-      ra[q] = (i < g.M && p < g.K) ? g.A[(int64_t)i * g.lda + p] : 0.0;
+      const bool ok = i < g.M && p < g.K;
+      cp_async8(as + ar * KST + ak + q, ok ? g.A + (int64_t)i * g.lda + p : g.A, ok);
     }
     if (TB == 1) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int j = j0 + ar, p = k0 + ak + q;
-        rb[q] = (j < g.N && p < g.K) ? g.B[(int64_t)j * g.ldb + p] : 0.0;
+        const bool ok = j < g.N && p < g.K;
+        cp_async8(bs + ar * KST + ak + q, ok ? g.B + (int64_t)j * g.ldb + p : g.B, ok);
       }
     } else {
 #pragma unroll
-      for (int h = 0; h < 4; ++h)
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int j = j0 + bj + 16 * h + e, p = k0 + bkr;
-          rb[2 * h + e] = (j < g.N && p < g.K) ? g.B[(int64_t)p * g.ldb + j] : 0.0;
-        }
-    }
-  };
-  auto sstore = [&](int buf) {
-#pragma unroll
-    for (int q = 0; q < 8; ++q) As[buf][ak + q][ar] = ra[q];
-    if (TB == 1) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) Bs[buf][ak + q][ar] = rb[q];
-    } else {
-#pragma unroll
-      for (int h = 0; h < 4; ++h)
-        *reinterpret_cast<double2*>(&Bs[buf][bkr][bj + 16 * h]) = make_double2(rb[2 * h], rb[2 * h + 1]);
+      for (int q = 0; q < 8; ++q) {
+        const int j = j0 + bj + q, p = k0 + bkr;
+        const bool ok = j < g.N && p < g.K;
+        cp_async8(bs + bkr * NST + bj + q, ok ? g.B + (int64_t)p * g.ldb + j : g.B, ok);
+      }
     }
   };
 
@@ -120,33 +128,37 @@ __global__ void __launch_bounds__(GT) dgemm_kernel(DGemm g) {
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 
-  int buf = 0;
-  if (kbeg < kend) {
-    gload(kbeg);
-    sstore(0);
-    __syncthreads();
+#pragma unroll
+  for (int s = 0; s < NSTAGE - 1; ++s) {
+    if (s < nk) issue(s, kbeg + s * GK);
+    cp_async_commit();
   }
-  for (int k0 = kbeg; k0 < kend; k0 += GK) {
-    const bool more = k0 + GK < kend;
-    if (more) gload(k0 + GK);
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<NSTAGE - 2>();  // this thread's copies of stage kt have landed
+    __syncthreads();              // everyone's have, and stage kt - 1 is consumed
+    if (kt + NSTAGE - 1 < nk) issue((kt + NSTAGE - 1) % NSTAGE, kbeg + (kt + NSTAGE - 1) * GK);
+    cp_async_commit();
+    const double* as = As + (kt % NSTAGE) * A_STAGE;
+    const double* bs = Bs + (kt % NSTAGE) * BSTG;
 #pragma unroll
     for (int kq = 0; kq < GK / 4; ++kq) {
       // fragments: A[row = lane/4][k = lane%4], B[k = lane%4][col = lane/4]
       const int kk = kq * 4 + (lane & 3);
       double af[4], bf[4];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) af[a] = As[buf][kk][wm * 32 + a * 8 + (lane >> 2)];
+      for (int a = 0; a < 4; ++a) af[a] = as[(wm * 32 + a * 8 + (lane >> 2)) * KST + kk];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) bf[b] = Bs[buf][kk][wn * 32 + b * 8 + (lane >> 2)];
+      for (int b = 0; b < 4; ++b) {
+        const int nn = wn * 32 + b * 8 + (lane >> 2);
+        bf[b] = TB ? bs[nn * KST + kk] : bs[kk * NST + nn];
+      }
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) dmma_m8n8k4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
     }
-    if (more) sstore(buf ^ 1);
-    __syncthreads();
-    buf ^= 1;
   }
+  cp_async_wait<0>();
 
   // accumulator fragment: row = lane/4, columns 2*(lane%4) + {0, 1}
 #pragma unroll
@@ -169,15 +181,22 @@ __global__ void __launch_bounds__(GT) dgemm_kernel(DGemm g) {
 cudaError_t dgemm(const DGemm& g, int tb, cudaStream_t s) {
   if (g.M <= 0 || g.N <= 0) return cudaSuccess;
   const dim3 grid(div_up(g.N, GN), div_up(g.M, GM));
-  if (tb == 0) dgemm_kernel<0><<<grid, GT, 0, s>>>(g);
-  else dgemm_kernel<1><<<grid, GT, 0, s>>>(g);
+  const size_t smem = sizeof(double) * NSTAGE * (A_STAGE + (tb ? B_STAGE_T : B_STAGE_N));
+  static bool attr_done[2] = {false, false};
+  if (!attr_done[tb]) {
+    if (tb == 0) cudaFuncSetAttribute(dgemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    else cudaFuncSetAttribute(dgemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_done[tb] = true;
+  }
+  if (tb == 0) dgemm_kernel<0><<<grid, GT, smem, s>>>(g);
+  else dgemm_kernel<1><<<grid, GT, smem, s>>>(g);
   return sf_launched(1);
 }
 
 // One warp factors the m x m (m <= 32) diagonal block at offset o of A
 // (right-looking, lane i holding row i in registers, the pivot column
-// broadcast through shared memory, scaled by the pivot's reciprocal as
-// LAPACK's potf2 does) and writes its inverse into Li.  A non-positive or
+// broadcast through shared memory and scaled by the reciprocal square root of
+// the pivot) and writes its inverse into Li.  A non-positive or
 // non-finite pivot records o + j + 1 in *info (first one wins) and continues
 // with pivot 1 so the kernel stays finite.
 __global__ void __launch_bounds__(32) chol_inv_leaf_kernel(const double* __restrict__ A, double* __restrict__ Li,
@@ -200,8 +219,8 @@ __global__ void __launch_bounds__(32) chol_inv_leaf_kernel(const double* __restr
       d = 1.0;
       if (lane == 0) atomicCAS(info, 0, o + j + 1);
     }
-    const double sd = sqrt(d);
-    const double rs = 1.0 / sd;
+    const double rs = rsqrt(d);  // one long-latency op per pivot on the serial chain
+    const double sd = d * rs;
     const double l = (lane > j) ? row[j] * rs : 0.0;
     if (lane == j) row[j] = sd;
     if (lane > j) row[j] = l;
@@ -218,14 +237,15 @@ __global__ void __launch_bounds__(32) chol_inv_leaf_kernel(const double* __restr
   __syncwarp();
   dinv[lane] = 1.0 / S[lane][lane];
   __syncwarp();
-  // lane c computes column c of L^{-1}: x[r] = (delta_rc - sum_{p<r} L[r][p] x[p]) / L[r][r]
+  // lane c computes column c of L^{-1}: x[r] = (delta_rc - sum_{p<r} L[r][p] x[p]) / L[r][r],
+  // the sum split over four independent partial sums to shorten the FMA chain
   double x[32];
 #pragma unroll
   for (int r = 0; r < 32; ++r) {
-    double acc = (r == lane) ? 1.0 : 0.0;
+    double acc[4] = {(r == lane) ? 1.0 : 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int p = 0; p < r; ++p) acc = fma(-S[r][p], x[p], acc);
-    x[r] = acc * dinv[r];
+    for (int p = 0; p < r; ++p) acc[p & 3] = fma(-S[r][p], x[p], acc[p & 3]);
+    x[r] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) * dinv[r];
   }
   if (lane < m) {
 #pragma unroll

@@ -23,6 +23,9 @@
 #include <chrono>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -184,10 +187,24 @@ void fine_apply(Mesh& m, DType t, Epi epi, const void* E, const void* u, const E
   SF_CUDA(launch_fine(t, epi, m.g, sh, E, m.mask.as<uint8_t>(), u, ea, s));
 }
 
-// Tuner: time candidate sweep shapes on this mesh and keep the fastest.
+// Tuner: time candidate sweep shapes on this mesh and keep the fastest.  The
+// choice is cached per process by grid size and precision, so every mesh of a
+// size runs the same kernels (identical results across handles, and handles
+// tuned while other streams are busy cannot pick a different shape).
+static std::mutex g_tune_mutex;
+static std::map<std::tuple<int, int, int, int>, SweepShape> g_tuned;
+
 void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
   const int idx = t == F64 ? 0 : 1;
   if (m.tuned[idx]) return;
+  std::lock_guard<std::mutex> lk(g_tune_mutex);
+  const auto key = std::make_tuple(m.g.nx, m.g.ny, m.g.nz, idx);
+  const auto hit = g_tuned.find(key);
+  if (hit != g_tuned.end()) {
+    m.sh[idx] = hit->second;
+    m.tuned[idx] = true;
+    return;
+  }
   const int maxt = t == F64 ? 256 : 512;
   const size_t es = dsize(t == BF16 ? F32 : t);
   DevBuf E, u, y;
@@ -248,6 +265,7 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
   cudaEventDestroy(e1);
   m.sh[idx] = best_sh;
   m.tuned[idx] = true;
+  g_tuned[key] = best_sh;
 }
 
 // ----------------------------------------------------------------------------

@@ -26,40 +26,54 @@ __device__ __forceinline__ int64_t node_id(const Grid& g, int i, int j, int k) {
   return ((int64_t)i * (g.ny + 1) + j) * (g.nz + 1) + k;
 }
 
+template <typename VT, typename CT>
+__device__ __forceinline__ VT coef_to(CT c) {
+  return (VT)to_d(c);
+}
+template <>
+__device__ __forceinline__ float coef_to<float, __nv_bfloat16>(__nv_bfloat16 c) {
+  return __bfloat162float(c);
+}
+
+// One thread per (node, output component r): 81 coefficient loads (coalesced
+// across the warp's consecutive nodes) and 81 gathered vector loads.  A
+// neighbour outside the grid has zero coefficients (the assembly writes them),
+// so its offset is clamped to 0 instead of branching and every load of the
+// thread can be in flight at once.  32-bit node indices (levels >= 1 have at
+// most 1/8 of the fine nodes; the launcher checks 3 * nn < 2^31).
 template <typename VT, typename CT, int EPI>
-__global__ void stencil_kernel(Grid g, const CT* __restrict__ coef, const uint8_t* __restrict__ mask,
-                               const VT* __restrict__ u, EpiArgs ea) {
+__global__ void __launch_bounds__(256) stencil_kernel(Grid g, const CT* __restrict__ coef,
+                                                      const uint8_t* __restrict__ mask, const VT* __restrict__ u,
+                                                      EpiArgs ea) {
   if (guard_off(ea.guard)) return;
-  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= g.nn) return;
-  int i, j, k;
-  node_ijk(g, n, i, j, k);
-  VT acc0 = 0, acc1 = 0, acc2 = 0;
+  const int nn = (int)g.nn;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (n >= nn) return;
+  const int NZ1 = g.nz + 1, NY1 = g.ny + 1;
+  const int k = n % NZ1, jq = n / NZ1;
+  const int j = jq % NY1, i = jq / NY1;
+  const int sx[3] = {i > 0 ? -NY1 * NZ1 : 0, 0, i < g.nx ? NY1 * NZ1 : 0};
+  const int sy[3] = {j > 0 ? -NZ1 : 0, 0, j < g.ny ? NZ1 : 0};
+  const int sz[3] = {k > 0 ? -1 : 0, 0, k < g.nz ? 1 : 0};
+  const CT* cp = coef + (int64_t)(r * 3) * nn + n;
+  VT acc = VT(0);
 #pragma unroll
   for (int o = 0; o < 27; ++o) {
-    const int dx = o / 9 - 1, dy = (o / 3) % 3 - 1, dz = o % 3 - 1;
-    const int ii = i + dx, jj = j + dy, kk = k + dz;
-    if (ii < 0 || jj < 0 || kk < 0 || ii > g.nx || jj > g.ny || kk > g.nz) continue;
-    const int64_t m = node_id(g, ii, jj, kk);
-    const VT u0 = u[3 * m], u1 = u[3 * m + 1], u2 = u[3 * m + 2];
-    const CT* cp = coef + (int64_t)o * 9 * g.nn + n;
-    acc0 += (VT)to_d(cp[0 * g.nn]) * u0 + (VT)to_d(cp[1 * g.nn]) * u1 + (VT)to_d(cp[2 * g.nn]) * u2;
-    acc1 += (VT)to_d(cp[3 * g.nn]) * u0 + (VT)to_d(cp[4 * g.nn]) * u1 + (VT)to_d(cp[5 * g.nn]) * u2;
-    acc2 += (VT)to_d(cp[6 * g.nn]) * u0 + (VT)to_d(cp[7 * g.nn]) * u1 + (VT)to_d(cp[8 * g.nn]) * u2;
-  }
-  const VT accs[3] = {acc0, acc1, acc2};
+    const VT* um = u + 3 * (n + sx[o / 9] + sy[(o / 3) % 3] + sz[o % 3]);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const int64_t dof = 3 * n + c;
-    epilogue<VT, EPI>(ea, dof, mask[dof] != 0, accs[c], u[dof]);
+    for (int q = 0; q < 3; ++q) acc += coef_to<VT, CT>(cp[(int64_t)(o * 9 + q) * nn]) * um[q];
   }
+  const int dof = 3 * n + r;
+  epilogue<VT, EPI>(ea, dof, mask[dof] != 0, acc, u[dof]);
 }
 
 template <typename VT, typename CT>
 static cudaError_t stencil_dispatch(Epi epi, const Grid& g, const void* coef, const uint8_t* mask,
                                     const void* u, const EpiArgs& ea, cudaStream_t s) {
-  const int bs = 128;
-  const int nb = div_up(g.nn, bs);
+  if (3 * g.nn >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
+  const int bs = 256;
+  const dim3 nb(div_up(g.nn, bs), 3);
   const CT* c = (const CT*)coef;
   const VT* uu = (const VT*)u;
   switch (epi) {

@@ -7,6 +7,8 @@ numbering and then dropped (the CUDA operator computes node indices).
 
 from __future__ import annotations
 
+import contextlib
+import contextvars
 import ctypes
 import hashlib
 
@@ -81,10 +83,26 @@ class NativeMesh:
                 pass
 
 
+# A mesh handle holds scratch vectors and the reduction workspace its
+# operators use, so handles shared between solvers must not run concurrently.
+# Solvers meant to run at the same time (BatchedFloorPolicy workers) build
+# their operators inside ``mesh_namespace(tag)`` and get private handles.
+_NAMESPACE = contextvars.ContextVar("simpfem_mesh_namespace", default=None)
+
+
+@contextlib.contextmanager
+def mesh_namespace(tag):
+    token = _NAMESPACE.set(tag)
+    try:
+        yield
+    finally:
+        _NAMESPACE.reset(token)
+
+
 def get_mesh(dims, free, ke=None) -> NativeMesh:
     free = np.ascontiguousarray(to_numpy(free), dtype=np.int32)
     ke = KE_UNIT_3D if ke is None else np.asarray(to_numpy(ke), dtype=np.float64)
-    key = (tuple(int(d) for d in dims), hashlib.sha1(free.tobytes()).hexdigest(),
+    key = (_NAMESPACE.get(), tuple(int(d) for d in dims), hashlib.sha1(free.tobytes()).hexdigest(),
            hashlib.sha1(np.ascontiguousarray(ke).tobytes()).hexdigest())
     m = _MESHES.get(key)
     if m is None:

@@ -15,6 +15,7 @@ recomputed from x after the solve.
 
 from __future__ import annotations
 
+import threading
 import time
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
@@ -22,6 +23,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
+from ._native import mesh_namespace
 from .multigrid_v4 import _cupy_fgmres
 from .paper4 import CANONICAL_STACK, _build_components
 
@@ -96,10 +98,13 @@ class GuardedFloorPolicy:
                        x0=None) -> FloorAttempt:
         torch = _lib.require_cuda()
         E_e = self.moduli(density, rho_min, binary=binary)
-        torch.cuda.synchronize()
+        # timing syncs wait for this policy's stream only, so policies on other
+        # streams (BatchedFloorPolicy) keep running
+        stream = torch.cuda.current_stream()
+        stream.synchronize()
         t0 = time.perf_counter()
         self.gmg.setup(E_e)
-        torch.cuda.synchronize()
+        stream.synchronize()
         setup_time = time.perf_counter() - t0
 
         def A_op(x):
@@ -108,7 +113,7 @@ class GuardedFloorPolicy:
         t0 = time.perf_counter()
         x, iters, reported = _cupy_fgmres(A_op, self.F_free_gpu, self.gmg.apply, x0=x0, tol=self.tol,
                                           maxiter=maxiter, restart=self.restart, history=history)
-        torch.cuda.synchronize()
+        stream.synchronize()
         solve_time = time.perf_counter() - t0
         final = float(torch.linalg.norm(self.F_free_gpu - A_op(x)) / self.b_norm)
         self.last_x = x
@@ -192,3 +197,66 @@ class GuardedFloorPolicy:
             "probe_history": probe_history,
             "attempts": attempts,
         }
+
+
+class BatchedFloorPolicy:
+    """Several density states in flight at once on one GPU.
+
+    ``width`` independent GuardedFloorPolicy workers, each with its own
+    hierarchy and CUDA stream, are driven by one host thread each (the library
+    releases the interpreter lock inside every call and synchronises only its
+    own stream).  While one state's hierarchy setup runs its latency-bound
+    coarsest factorisation, the other states' cycles fill the GPU.  State k goes
+    to worker k mod width and each worker takes its states in order, so results
+    are deterministic; every worker carries its own lambda-cache history, as one
+    driver hierarchy does.  Every accepted answer still passes the FP64 guard.
+    """
+
+    def __init__(self, width: int = 3, *args, **kwargs):
+        torch = _lib.require_cuda()
+        if int(width) < 1:
+            raise ValueError("width must be >= 1")
+        self.width = int(width)
+        self.workers = []
+        for i in range(self.width):
+            # private mesh handles: scratch and reduction workspaces are per handle
+            with mesh_namespace(("batched", id(self), i)):
+                self.workers.append(GuardedFloorPolicy(*args, **kwargs))
+        self.streams = [torch.cuda.Stream() for _ in range(self.width)]
+        # pick the sweep shapes now, on an idle device; every worker's mesh (same
+        # grid) then reuses them
+        _lib.call("simpfem_mesh_tune", self.workers[0].mf_op.mesh.handle, _lib.stream_ptr())
+        torch.cuda.current_stream().synchronize()
+
+    def run_many(self, densities, *, binary: bool = False, on_result=None) -> list:
+        """Run the policy on every state; returns the result rows in input order.
+        ``on_result(k, worker, row)`` runs on the worker's thread and stream right
+        after state k finishes (e.g. to copy ``worker.last_x`` to the host)."""
+        torch = _lib.require_cuda()
+        n = len(densities)
+        rows: list = [None] * n
+        errors: list = []
+        caller = torch.cuda.current_stream()
+        for s in self.streams:
+            s.wait_stream(caller)  # inputs prepared on the caller's stream are visible
+
+        def work(i: int) -> None:
+            try:
+                with torch.cuda.stream(self.streams[i]):
+                    for k in range(i, n, self.width):
+                        rows[k] = self.workers[i].run(densities[k], binary=binary)
+                        if on_result is not None:
+                            on_result(k, self.workers[i], rows[k])
+            except BaseException as e:  # re-raised on the calling thread
+                errors.append(e)
+
+        threads = [threading.Thread(target=work, args=(i,)) for i in range(min(self.width, n))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for s in self.streams:
+            caller.wait_stream(s)
+        if errors:
+            raise errors[0]
+        return rows

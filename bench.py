@@ -79,7 +79,9 @@ def _stack(name: str, precision: str) -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """SM clocks and throttle reasons sampled every 200 ms while running: NVML
+    queries in-process (no child process is started inside the timed region),
+    nvidia-smi only when NVML is not importable."""
 
     def __init__(self, index: int):
         self.index = index
@@ -87,7 +89,37 @@ class ClockSampler:
         self._stop = threading.Event()
         self._t = threading.Thread(target=self._run, daemon=True)
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
     def _run(self):
+        try:
+            nv, h = self._nvml_handle()
+        except Exception:
+            nv = None
+        if nv is not None:
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            while not self._stop.is_set():
+                try:
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append([str(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                         str(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                                         str(nv.nvmlDeviceGetPowerUsage(h) / 1000.0)]
+                                        + ["Active" if r & b else "Not Active" for b in bits])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+            return
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")

@@ -162,8 +162,9 @@ int simpfem_gmg_apply(simpfem_gmg* g, const double* rhs_free, double* z_free, vo
 int simpfem_gmg_props_get(simpfem_gmg* g, simpfem_gmg_props* out);
 /* Average device time (ms) of one fused smoothing step of `level` (below the
  * coarsest) -- the operator kernel with the smoother's update fused into its
- * store, the kernel the cycle launches most -- over `reps` launches timed with CUDA
- * events on `stream`; clobbers that level's cycle vectors (no reference
+ * store, the kernel the cycle launches most -- over `reps` launches, each timed by
+ * its own CUDA event pair on `stream` after a 256 MB write that evicts the L2, on
+ * pseudo-random input vectors; clobbers that level's cycle vectors (no reference
  * counterpart: instrumentation for the roofline report). */
 int simpfem_gmg_time_smoother_step(simpfem_gmg* g, int level, int reps, float* avg_ms, void* stream);
 /* Forget the cached lambda_max estimates (the next setup re-estimates). */

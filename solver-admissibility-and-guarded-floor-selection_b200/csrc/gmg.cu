@@ -211,7 +211,7 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
   E.alloc(es * std::max<int64_t>(1, m.g.ne()));
   u.alloc(es * m.g.ndof);
   y.alloc(es * m.g.ndof);
-  SF_CUDA(cudaMemsetAsync(u.p, 0, es * m.g.ndof, s));
+  SF_CUDA(launch_fill_hash(t == F64 ? F64 : F32, m.g.ndof, 7u, u.p, s));
   SF_CUDA(launch_fill(t == F64 ? F64 : F32, m.g.ne(), 1.0, E.p, nullptr, s));
   std::vector<SweepShape> cands;
   std::vector<int> bks;
@@ -1257,9 +1257,10 @@ float time_smoother_step(Gmg& G, int l, int reps) {
   void* rhs = vt == t ? L.rhs.p : L.rhss.p;
   void* d = vt == t ? L.d.p : L.ds.p;
   const size_t es = vt == F64 ? 8 : 4;
-  SF_CUDA(cudaMemsetAsync(x, 0, es * L.g.ndof, G.st));
-  SF_CUDA(cudaMemsetAsync(rhs, 0, es * L.g.ndof, G.st));
-  SF_CUDA(cudaMemsetAsync(d, 0, es * L.g.ndof, G.st));
+  // non-constant inputs, so the timed step moves data like a real cycle does
+  SF_CUDA(launch_fill_hash(vt, L.g.ndof, 11u, x, G.st));
+  SF_CUDA(launch_fill_hash(vt, L.g.ndof, 12u, rhs, G.st));
+  SF_CUDA(launch_fill_hash(vt, L.g.ndof, 13u, d, G.st));
   EpiArgs ea;
   ea.b = rhs;
   ea.dinv = level_dinv(G, l, vt);
@@ -1271,18 +1272,28 @@ float time_smoother_step(Gmg& G, int l, int reps) {
   const int psel = (vt == F32) ? p : F64;
   G.guard = nullptr;
   level_op(G, l, vt, psel, epi, x, ea);
-  cudaEvent_t e0, e1;
-  SF_CUDA(cudaEventCreate(&e0));
-  SF_CUDA(cudaEventCreate(&e1));
-  SF_CUDA(cudaEventRecord(e0, G.st));
-  for (int r = 0; r < reps; ++r) level_op(G, l, vt, psel, epi, x, ea);
-  SF_CUDA(cudaEventRecord(e1, G.st));
-  SF_CUDA(cudaEventSynchronize(e1));
-  float ms = 0.f;
-  SF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  return ms / reps;
+  // each rep starts from a cold L2: a 256 MB buffer (twice the L2) is written
+  // between reps, and only the step itself is inside its event pair
+  DevBuf flush;
+  const size_t flush_bytes = size_t(256) << 20;
+  flush.alloc(flush_bytes);
+  std::vector<cudaEvent_t> ev(2 * reps);
+  for (auto& e : ev) SF_CUDA(cudaEventCreate(&e));
+  for (int r = 0; r < reps; ++r) {
+    SF_CUDA(cudaMemsetAsync(flush.p, r & 0xff, flush_bytes, G.st));
+    SF_CUDA(cudaEventRecord(ev[2 * r], G.st));
+    level_op(G, l, vt, psel, epi, x, ea);
+    SF_CUDA(cudaEventRecord(ev[2 * r + 1], G.st));
+  }
+  SF_CUDA(cudaEventSynchronize(ev.back()));
+  float total = 0.f;
+  for (int r = 0; r < reps; ++r) {
+    float ms = 0.f;
+    SF_CUDA(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]));
+    total += ms;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return total / reps;
 }
 
 // Outer FGMRES: host-controlled (one synchronisation per iteration to read the

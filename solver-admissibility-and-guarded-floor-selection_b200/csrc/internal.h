@@ -156,6 +156,7 @@ cudaError_t launch_minmax_count(int64_t n, const double* E, double thr, RedWork 
 cudaError_t launch_axpby(DType t, int64_t n, double alpha, const void* x, double beta,
                          const void* y, void* out, const int* guard, cudaStream_t s);
 cudaError_t launch_fill(DType t, int64_t n, double v, void* out, const int* guard, cudaStream_t s);
+cudaError_t launch_fill_hash(DType t, int64_t n, uint32_t seed, void* out, cudaStream_t s);
 cudaError_t launch_copy(DType t, int64_t n, const void* src, void* dst, const int* guard,
                         cudaStream_t s);
 cudaError_t launch_cheb_zero(DType t, int64_t n, double alpha, const void* dinv, const void* rhs,

@@ -220,6 +220,28 @@ __global__ void fill_kernel(int64_t n, T v, T* __restrict__ out, const int* guar
   if (i < n) out[i] = v;
 }
 
+// out[i] = a pseudo-random value in [-0.5, 0.5) from a hash of (i, seed): test
+// data for timing kernels on realistic (non-constant) vectors.
+template <typename T>
+__global__ void fill_hash_kernel(int64_t n, uint32_t seed, T* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t h = (uint32_t)i * 2654435761u ^ (uint32_t)(i >> 32) ^ seed;
+  h ^= h >> 15;
+  h *= 0x2c1b3c6du;
+  h ^= h >> 12;
+  out[i] = (T)((double)(h & 0xffffffu) * (1.0 / 16777216.0) - 0.5);
+}
+
+cudaError_t launch_fill_hash(DType t, int64_t n, uint32_t seed, void* out, cudaStream_t s) {
+  const int nb = div_up(n, 256);
+  if (t == F64)
+    fill_hash_kernel<double><<<nb, 256, 0, s>>>(n, seed, (double*)out);
+  else
+    fill_hash_kernel<float><<<nb, 256, 0, s>>>(n, seed, (float*)out);
+  return sf_launched(1);
+}
+
 cudaError_t launch_fill(DType t, int64_t n, double v, void* out, const int* guard, cudaStream_t s) {
   const int nb = div_up(n, 256);
   if (t == F64)

@@ -334,7 +334,7 @@ def run_native(args):
         },
         "gpu_launches": int(launches),
         "roofline": {
-            "kernel": f"fine_sweep_kernel<float, {'JAC' if args.stack == 'plain' else 'CHEB'}> (fused smoothing step)",
+            "kernel": f"fine_sweep_x2_kernel<EPI_{'JAC' if args.stack == 'plain' else 'CHEB'}> (FP32 fused smoothing step, cold L2)",
             "bound": "hbm",
             "achieved": round(achieved, 1),
             "peak": hbm_peak,

@@ -63,6 +63,14 @@ def _make_cupy_module() -> types.ModuleType:
             return self._rs.standard_normal(n).astype(dtype)
 
     cp.random = types.SimpleNamespace(RandomState=_RS)
+
+    class _Scalar(np.ndarray):
+        """0-d result with CuPy's ``.get()`` (device -> host copy)."""
+
+        def get(self):
+            return np.asarray(self)
+
+    cp.dot = lambda a, b, out=None: np.asarray(np.dot(a, b)).view(_Scalar)
     return cp
 
 

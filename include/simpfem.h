@@ -180,6 +180,18 @@ int simpfem_gmg_fine_E(simpfem_gmg* g, const double** E_out);
 int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
                    double tol, int maxiter, int restart, double* history_host, int history_cap,
                    int* history_len, int* iters, int* converged, void* stream);
+/* simpfem_fgmres with a host check, no counterpart in the reference (the learned
+ * floor policy decides at the probe's r50 point with it): once the solve has
+ * completed check_iter iterations and is still running, check_fn(check_ctx,
+ * check_iter, history, history_len) is called on the calling thread with the
+ * relative-residual history so far; a nonzero return ends the solve there, with
+ * x_free the iterate after check_iter iterations, *converged 0 and *stopped 1.
+ * check_iter < 1 or check_fn NULL is simpfem_fgmres.  stopped may be NULL. */
+int simpfem_fgmres_checked(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
+                           double tol, int maxiter, int restart, double* history_host, int history_cap,
+                           int* history_len, int* iters, int* converged, int check_iter,
+                           int (*check_fn)(void* ctx, int iters, const double* history, int history_len),
+                           void* check_ctx, int* stopped, void* stream);
 /* PCG with the hierarchy as preconditioner (_cupy_pcg, gpu_fem/solver_v2.py:551-623). */
 int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
                 double tol, int maxiter, double* history_host, int history_cap, int* history_len,
@@ -193,6 +205,37 @@ int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, dou
  * *info_host: 0 on success, else the 1-based index of the first non-positive or
  * non-finite pivot, or n + 1 when L^{-1} holds a non-finite entry. */
 int simpfem_dense_cholesky_inverse(int n, double* A, double* Linv, int* info_host, void* stream);
+
+/* ---- learned floor proposer (no counterpart in the reference) ------------------
+ * A small 3D CNN over the density pooled to 16^3 plus two probe features, with a
+ * 3-way softmax over the floor rungs {1e-12, 1e-3, 1e-2}: conv 1->16 (stride 1),
+ * 16->16, 16->32, 32->32 (stride 2), 3x3x3, pad 1, ReLU; mean over the last 2^3;
+ * dense 34 -> 3.  Weights are used as bfloat16, everything else float32.
+ * Parameters (float32, simpfem_cnn_n_params() of them) in the order
+ * W1 b1 W2 b2 W3 b3 W4 b4 Wfc bfc, conv weights [cout][cin][kz][ky][kx]. */
+typedef struct simpfem_cnn simpfem_cnn;
+int simpfem_cnn_n_params(void);
+/* Workspaces for batches of up to max_batch samples; parameters start at zero. */
+int simpfem_cnn_create(int max_batch, simpfem_cnn** out);
+int simpfem_cnn_destroy(simpfem_cnn* h);
+/* Host parameter copies; set_params also resets the Adam moments and step count. */
+int simpfem_cnn_set_params(simpfem_cnn* h, const float* host, int n);
+int simpfem_cnn_get_params(simpfem_cnn* h, float* host, int n);
+/* Average-pool one device density field (nx, ny, nz elements, element index
+ * (i*ny + j)*nz + k, FP64) to the network input (16^3 float32, device); window i
+ * along an axis of n elements covers [floor(i*n/16), ceil((i+1)*n/16)). */
+int simpfem_cnn_pool16(int nx, int ny, int nz, const double* density, float* out, void* stream);
+/* prob (N x 3, device) <- softmax of the network on x (N x 16^3, device) and
+ * feats (N x 2, device); 1 <= N <= max_batch. */
+int simpfem_cnn_forward(simpfem_cnn* h, const float* x, const float* feats, int N, float* prob, void* stream);
+/* Mean cross-entropy against labels (N int32 in {0, 1, 2}, device) and its
+ * gradient with respect to every parameter, kept on the device for adam_step;
+ * grad_host (n_params) and loss_host (1) may be NULL, else they are filled and
+ * the call synchronises the stream.  Reductions run in a fixed order. */
+int simpfem_cnn_loss_grad(simpfem_cnn* h, const float* x, const float* feats, const int32_t* labels, int N,
+                          float* grad_host, float* loss_host, void* stream);
+/* One Adam update of the parameters with the last loss_grad gradient. */
+int simpfem_cnn_adam_step(simpfem_cnn* h, float lr, float beta1, float beta2, float eps, void* stream);
 
 #ifdef __cplusplus
 }

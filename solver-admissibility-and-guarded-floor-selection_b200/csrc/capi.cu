@@ -372,9 +372,11 @@ int simpfem_gmg_fine_E(simpfem_gmg* g, const double** E_out) {
   SF_API_END
 }
 
-int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free, double tol,
-                   int maxiter, int restart, double* history_host, int history_cap, int* history_len, int* iters,
-                   int* converged, void* stream) {
+int simpfem_fgmres_checked(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
+                           double tol, int maxiter, int restart, double* history_host, int history_cap,
+                           int* history_len, int* iters, int* converged, int check_iter,
+                           int (*check_fn)(void* ctx, int iters, const double* history, int history_len),
+                           void* check_ctx, int* stopped, void* stream) {
   SF_API_BEGIN
   if (!g || !b_free || !x_free) throw InvalidArg{"simpfem_fgmres: null argument"};
   if (restart < 1 || restart > 1000 || maxiter < 0) throw InvalidArg{"simpfem_fgmres: restart must be in [1, 1000]"};
@@ -391,8 +393,13 @@ int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, 
   G.hist_pin.alloc(sizeof(double) * cap);
   G.hist_dev.alloc(sizeof(double) * cap);
   PrecFn M = [&G](const double* in, double* out, const int* guard) { apply_full(G, in, out, guard); };
+  CheckHook hook;
+  hook.iter = check_iter;
+  hook.fn = check_iter >= 1 ? check_fn : nullptr;
+  hook.ctx = check_ctx;
   run_outer_fgmres(G, g->bfull.as<double>(), g->xfull.as<double>(), x0_free == nullptr, tol, maxiter, restart, M,
-                   G.hist_dev.as<double>(), cap);
+                   G.hist_dev.as<double>(), cap, &hook);
+  if (stopped) *stopped = hook.stopped ? 1 : 0;
   SF_CUDA(cudaMemcpyAsync(G.hist_pin.h, G.hist_dev.p, sizeof(double) * cap, cudaMemcpyDeviceToHost, G.st));
   SF_CUDA(cudaStreamSynchronize(G.st));
   const int* f = G.outer.hflags();
@@ -406,6 +413,13 @@ int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, 
   if (converged) *converged = f[F_CONV];
   SF_CUDA(launch_compress(F64, m.n_free, m.free_idx.as<int32_t>(), g->xfull.p, x_free, G.st));
   SF_API_END
+}
+
+int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free, double tol,
+                   int maxiter, int restart, double* history_host, int history_cap, int* history_len, int* iters,
+                   int* converged, void* stream) {
+  return simpfem_fgmres_checked(g, b_free, x0_free, x_free, tol, maxiter, restart, history_host, history_cap,
+                                history_len, iters, converged, -1, nullptr, nullptr, nullptr, stream);
 }
 
 int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free, double tol,

@@ -757,7 +757,7 @@ static void base_cycle(Gmg& G, const double* rhs, double* out) {
 
 static void fgmres(Gmg& G, KrylovWs& K, const double* b, double* x, bool x0_zero, double tol, int maxiter,
                    int restart, const PrecFn& M, const int* parent, bool host_control, double* hist_dev,
-                   int hist_cap) {
+                   int hist_cap, const CheckHook* check = nullptr) {
   const int64_t n = G.nfull();
   Mesh& m = *G.m;
   K.ensure(n, restart);
@@ -774,7 +774,8 @@ static void fgmres(Gmg& G, KrylovWs& K, const double* b, double* x, bool x0_zero
   SF_CUDA(launch_krylov_init(kd, parent, G.st));
   if (x0_zero) SF_CUDA(launch_fill(F64, n, 0.0, x, K.dflag(F_NOTDONE), G.st));
   const int ncycles = (maxiter + restart - 1) / std::max(restart, 1);
-  for (int c = 0; c < ncycles; ++c) {
+  bool stopped = false;
+  for (int c = 0; c < ncycles && !stopped; ++c) {
     if (host_control) {
       K.sync_flags(G.st);
       if (K.hflags()[F_DONE]) break;
@@ -821,6 +822,20 @@ static void fgmres(Gmg& G, KrylovWs& K, const double* b, double* x, bool x0_zero
       if (host_control) {
         K.sync_flags(G.st);
         if (!K.hflags()[F_CYC]) break;
+        // the caller's check at a fixed iteration count (the solve is still running):
+        // it sees the residual history so far and may end the solve here; the
+        // iterate after these columns is then formed as at the end of a cycle
+        if (check && check->fn && K.hflags()[F_TOTAL] == check->iter && hist_dev) {
+          const int hn = std::min(K.hflags()[F_HISTN], hist_cap);
+          check->buf.resize(hn);
+          SF_CUDA(cudaMemcpyAsync(check->buf.data(), hist_dev, sizeof(double) * hn, cudaMemcpyDeviceToHost, G.st));
+          SF_CUDA(cudaStreamSynchronize(G.st));
+          if (check->fn(check->ctx, check->iter, check->buf.data(), hn)) {
+            stopped = true;
+            check->stopped = true;
+            break;
+          }
+        }
       }
     }
     SF_CUDA(launch_backsolve(kd, G.st));
@@ -1299,8 +1314,8 @@ float time_smoother_step(Gmg& G, int l, int reps) {
 // Outer FGMRES: host-controlled (one synchronisation per iteration to read the
 // device-side convergence flags), history written straight into mapped memory.
 void run_outer_fgmres(Gmg& G, const double* b, double* x, bool x0_zero, double tol, int maxiter, int restart,
-                      const PrecFn& M, double* hist_dev, int hist_cap) {
-  fgmres(G, G.outer, b, x, x0_zero, tol, maxiter, restart, M, nullptr, true, hist_dev, hist_cap);
+                      const PrecFn& M, double* hist_dev, int hist_cap, const CheckHook* check) {
+  fgmres(G, G.outer, b, x, x0_zero, tol, maxiter, restart, M, nullptr, true, hist_dev, hist_cap, check);
   G.outer.sync_flags(G.st);
 }
 

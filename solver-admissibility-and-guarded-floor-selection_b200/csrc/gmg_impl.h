@@ -215,8 +215,18 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s);
 Gmg* gmg_create(Mesh* m, const simpfem_gmg_opts& o);
 void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free);
 void apply_full(Gmg& G, const double* rhs, double* out, const int* guard);
+// A host check called once, when the outer FGMRES has completed ``iter``
+// iterations and is still running: fn(ctx, iter, history, history_len) sees the
+// relative-residual history so far and returns nonzero to end the solve there.
+struct CheckHook {
+  int iter = -1;
+  int (*fn)(void* ctx, int iters, const double* history, int history_len) = nullptr;
+  void* ctx = nullptr;
+  mutable std::vector<double> buf;
+  mutable bool stopped = false;
+};
 void run_outer_fgmres(Gmg& G, const double* b, double* x, bool x0_zero, double tol, int maxiter, int restart,
-                      const PrecFn& M, double* hist_dev, int hist_cap);
+                      const PrecFn& M, double* hist_dev, int hist_cap, const CheckHook* check = nullptr);
 float time_smoother_step(Gmg& G, int l, int reps);
 void run_pcg(Gmg& G, const double* b, double* x, double tol, int maxiter, std::vector<double>* hist, int* iters,
              int* conv);

@@ -111,8 +111,18 @@ _SIGS = {
     "simpfem_gmg_reset_lambda_cache": (_I, [_P]),
     "simpfem_gmg_fine_E": (_I, [_P, _P]),
     "simpfem_fgmres": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _P]),
+    "simpfem_fgmres_checked": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _I, _P, _P, _P, _P]),
     "simpfem_pcg": (_I, [_P, _P, _P, _P, _D, _I, _P, _I, _P, _P, _P, _P]),
     "simpfem_dense_cholesky_inverse": (_I, [_I, _P, _P, _P, _P]),
+    "simpfem_cnn_n_params": (_I, []),
+    "simpfem_cnn_create": (_I, [_I, ctypes.POINTER(_P)]),
+    "simpfem_cnn_destroy": (_I, [_P]),
+    "simpfem_cnn_set_params": (_I, [_P, _P, _I]),
+    "simpfem_cnn_get_params": (_I, [_P, _P, _I]),
+    "simpfem_cnn_pool16": (_I, [_I, _I, _I, _P, _P, _P]),
+    "simpfem_cnn_forward": (_I, [_P, _P, _P, _I, _P, _P]),
+    "simpfem_cnn_loss_grad": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
+    "simpfem_cnn_adam_step": (_I, [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P]),
 }
 
 

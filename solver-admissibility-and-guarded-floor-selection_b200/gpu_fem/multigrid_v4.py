@@ -29,6 +29,9 @@ from ._native import to_numpy
 from .solver_v2 import MatrixFreeKff, _native_gmg
 
 _PREC = {"fp64": _lib.F64, "fp32": _lib.F32, "bf16": _lib.BF16}
+# int check(void* ctx, int iters, const double* history, int history_len)
+_CHECK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                             ctypes.c_int)
 _PREC_NAME = {v: k for k, v in _PREC.items()}
 _ENRICH = {"none": 0, "weighted_residual_second": 1, "weighted_gap_second": 2, "void_residual_second": 3,
            "void_gap_second": 4}
@@ -399,7 +402,10 @@ class GalerkinMatFreeGMG:
         return self._kappa_eff
 
     # ------------------------------------------------------------ native Krylov
-    def _native_fgmres(self, b, x0, tol, maxiter, restart, history):
+    def _native_fgmres(self, b, x0, tol, maxiter, restart, history, check=None):
+        """``check``: optional (iteration, fn); fn(history_so_far) runs once when the
+        solve has completed that many iterations and is still running, and a true
+        return ends the solve there (the result then reports not converged)."""
         torch = _lib.require_cuda()
         bb = _lib.as_cuda(b, torch.float64)
         x = torch.empty_like(bb)
@@ -407,9 +413,31 @@ class GalerkinMatFreeGMG:
         cap = int(maxiter) + int(maxiter) // max(int(restart), 1) + 4
         hist = np.zeros(cap, dtype=np.float64)
         hlen, it, conv = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _lib.call("simpfem_fgmres", self._h, _lib.ptr(bb), _lib.ptr(x0t) if x0t is not None else None, _lib.ptr(x),
-                  float(tol), int(maxiter), int(restart), hist.ctypes.data_as(ctypes.c_void_p), cap,
-                  ctypes.byref(hlen), ctypes.byref(it), ctypes.byref(conv), _lib.stream_ptr())
+        self.last_stopped = False
+        if check is None:
+            _lib.call("simpfem_fgmres", self._h, _lib.ptr(bb), _lib.ptr(x0t) if x0t is not None else None,
+                      _lib.ptr(x), float(tol), int(maxiter), int(restart), hist.ctypes.data_as(ctypes.c_void_p), cap,
+                      ctypes.byref(hlen), ctypes.byref(it), ctypes.byref(conv), _lib.stream_ptr())
+        else:
+            check_iter, fn = check
+            errors = []
+
+            def trampoline(_ctx, _iters, hptr, hn):
+                try:
+                    return 1 if fn([float(hptr[k]) for k in range(hn)]) else 0
+                except BaseException as e:  # raised again once the call returns
+                    errors.append(e)
+                    return 0
+
+            cb = _CHECK_FN(trampoline)
+            stopped = ctypes.c_int()
+            _lib.call("simpfem_fgmres_checked", self._h, _lib.ptr(bb), _lib.ptr(x0t) if x0t is not None else None,
+                      _lib.ptr(x), float(tol), int(maxiter), int(restart), hist.ctypes.data_as(ctypes.c_void_p), cap,
+                      ctypes.byref(hlen), ctypes.byref(it), ctypes.byref(conv), int(check_iter),
+                      ctypes.cast(cb, ctypes.c_void_p), None, ctypes.byref(stopped), _lib.stream_ptr())
+            if errors:
+                raise errors[0]
+            self.last_stopped = bool(stopped.value)
         if history is not None:
             history.extend(float(v) for v in hist[: min(hlen.value, cap)])
         return x, int(it.value), bool(conv.value)

@@ -95,7 +95,10 @@ class GuardedFloorPolicy:
         return rho_min + (1.0 - rho_min) * rho ** self.penal
 
     def solve_at_floor(self, density, rho_min: float, *, maxiter: int, history: list, binary: bool = False,
-                       x0=None) -> FloorAttempt:
+                       x0=None, check=None) -> FloorAttempt:
+        """One guarded solve at ``rho_min``.  ``check`` (iteration, fn): fn(history so
+        far) runs once the solve has done that many iterations and may end it there
+        (the learned floor policy's decision point; the plain policy passes none)."""
         torch = _lib.require_cuda()
         E_e = self.moduli(density, rho_min, binary=binary)
         # timing syncs wait for this policy's stream only, so policies on other
@@ -111,8 +114,12 @@ class GuardedFloorPolicy:
             return self.mf_op.matvec(x, E_e)
 
         t0 = time.perf_counter()
-        x, iters, reported = _cupy_fgmres(A_op, self.F_free_gpu, self.gmg.apply, x0=x0, tol=self.tol,
-                                          maxiter=maxiter, restart=self.restart, history=history)
+        if check is None:
+            x, iters, reported = _cupy_fgmres(A_op, self.F_free_gpu, self.gmg.apply, x0=x0, tol=self.tol,
+                                              maxiter=maxiter, restart=self.restart, history=history)
+        else:
+            x, iters, reported = self.gmg._native_fgmres(self.F_free_gpu, x0, self.tol, maxiter, self.restart,
+                                                         history, check=check)
         stream.synchronize()
         solve_time = time.perf_counter() - t0
         final = float(torch.linalg.norm(self.F_free_gpu - A_op(x)) / self.b_norm)

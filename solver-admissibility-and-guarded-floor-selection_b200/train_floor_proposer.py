@@ -1,6 +1,6 @@
 """Generate, label, train and evaluate the learned floor proposer on one GPU.
 
-    python train_floor_proposer.py [--train 4096] [--heldout 512] [--epochs 40] [--out gpu_fem/data]
+    python train_floor_proposer.py [--train 4096] [--val 512] [--heldout 512] [--epochs 30] [--out gpu_fem/data]
 
 States: cantilever meshes 40x20x20 and 80x40x20, elements void with probability
 p (seeded Bernoulli); half the states are cone-filtered with p ~ U[0.1, 0.6] and
@@ -13,9 +13,11 @@ FGMRES restart 300, tol 1e-6; gpu_fem.policy.BatchedFloorPolicy) and labelled
 with the rung that policy selects; the features are the density pooled to 16^3,
 the probe's r50 and the iteration at which it reached 1e-2.  The network is
 trained with the library's own CUDA forward/backward kernels (class-balanced
-mini-batch Adam); then the held-out states are solved one at a time by the plain
-policy and by LearnedFloorPolicy and compared: floor attempts, setups, outer
-iterations, policy time, selected floor, guarded answers.  Writes
+mini-batch Adam) on all but the last --val training states, which choose the
+epoch (lowest validation loss).  The held-out states are then solved one at a
+time by the plain policy, by the r50 rule stop alone (no network) and by
+LearnedFloorPolicy, and compared: floor attempts, setups, outer iterations,
+policy time, selected floor, guarded answers.  Writes
 floor_proposer.npz (parameters) and floor_proposer_eval.json (dataset, training
 curve, held-out comparison).
 """
@@ -109,56 +111,66 @@ def features(states, rows):
 
 
 def evaluate(net, held):
-    """Held-out states through the plain and the learned policy, one state at a
-    time on one stream each (same hierarchy configuration), in the same order."""
+    """Held-out states through three policies, one state at a time on one stream
+    each (same hierarchy configuration, same order): the plain policy; the r50
+    rule stop alone (LearnedFloorPolicy with a proposer that always says rung 0,
+    so the probe stops at r50 only when r50 is above the high threshold); and the
+    learned policy with the trained network."""
     import torch
 
-    from gpu_fem.floor_proposer import LearnedFloorPolicy
+    from gpu_fem.floor_proposer import FloorProposerNet, LearnedFloorPolicy
     from gpu_fem.policy import GuardedFloorPolicy
     from gpu_fem.presets import cantilever_spec
 
-    plain_rows, learned_rows = [None] * len(held), [None] * len(held)
+    zero = FloorProposerNet(max_batch=4, params=np.zeros(net.n_params, dtype=np.float32))
+    rows = {"plain": [None] * len(held), "rule": [None] * len(held), "learned": [None] * len(held)}
     for dims in MESHES:
         idx = [i for i, s in enumerate(held) if s["dims"] == dims]
         if not idx:
             continue
         spec = cantilever_spec(*dims)
-        plain = GuardedFloorPolicy(spec, stack=_stack(), **POLICY)
-        learned = LearnedFloorPolicy(spec, proposer=net, dims=dims, stack=_stack(), **POLICY)
+        pols = {"plain": GuardedFloorPolicy(spec, stack=_stack(), **POLICY),
+                "rule": LearnedFloorPolicy(spec, proposer=zero, dims=dims, stack=_stack(), **POLICY),
+                "learned": LearnedFloorPolicy(spec, proposer=net, dims=dims, stack=_stack(), **POLICY)}
         for i in idx:
             d = torch.as_tensor(held[i]["density"], device="cuda")
-            plain_rows[i] = plain.run(d)
-            learned_rows[i] = learned.run(d)
-    return plain_rows, learned_rows
+            for k, pol in pols.items():
+                rows[k][i] = pol.run(d)
+    return rows
 
 
-def compare(plain_rows, learned_rows, mask=None):
-    sel = [k for k in range(len(plain_rows)) if mask is None or mask[k]]
-    P = [plain_rows[k] for k in sel]
-    L = [learned_rows[k] for k in sel]
+def compare(rows, mask=None):
+    """Totals per policy over the states in ``mask`` (all by default); floors are
+    compared with the plain policy's selection."""
+    plain = rows["plain"]
+    sel = [k for k in range(len(plain)) if mask is None or mask[k]]
 
-    def tot(rows, key):
-        return float(np.sum([r[key] for r in rows]))
+    def tot(arm, key):
+        return float(np.sum([rows[arm][k][key] for k in sel]))
 
-    return {
-        "states": len(sel),
-        "floor_attempts": [tot(P, "n_floor_attempts"), tot(L, "n_floor_attempts")],
-        "setups": [tot(P, "n_setups"), tot(L, "n_setups")],
-        "outer_iterations": [tot(P, "total_iters"), tot(L, "total_iters")],
-        "policy_time_s": [tot(P, "recorded_policy_time_s"), tot(L, "policy_time_s")],
-        "same_selected_floor": float(np.mean([p["recommended_rho_min"] == q["recommended_rho_min"]
-                                              for p, q in zip(P, L)])) if sel else float("nan"),
-        "higher_floor_than_plain": int(sum(q["recommended_rho_min"] > p["recommended_rho_min"] for p, q in zip(P, L))),
-        "lower_floor_than_plain": int(sum(q["recommended_rho_min"] < p["recommended_rho_min"] for p, q in zip(P, L))),
-        "guarded": [int(sum(r["solve_converged"] for r in P)), int(sum(r["solve_converged"] for r in L))],
-    }
+    out = {"states": len(sel)}
+    for arm in rows:
+        tkey = "recorded_policy_time_s" if arm == "plain" else "policy_time_s"
+        out[arm] = {
+            "floor_attempts": tot(arm, "n_floor_attempts"),
+            "setups": tot(arm, "n_setups"),
+            "outer_iterations": tot(arm, "total_iters"),
+            "policy_time_s": tot(arm, tkey),
+            "guarded": int(tot(arm, "solve_converged")),
+            "same_floor_as_plain": int(sum(rows[arm][k]["recommended_rho_min"] == plain[k]["recommended_rho_min"]
+                                           for k in sel)),
+            "higher_floor_than_plain": int(sum(rows[arm][k]["recommended_rho_min"] > plain[k]["recommended_rho_min"]
+                                               for k in sel)),
+        }
+    return out
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=4096)
     ap.add_argument("--heldout", type=int, default=512)
-    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--val", type=int, default=512)
     ap.add_argument("--width", type=int, default=4)
     ap.add_argument("--out", default=os.path.join(HERE, "gpu_fem", "data"))
     a = ap.parse_args()
@@ -174,38 +186,54 @@ def main() -> None:
     rows_train = solve_plain(train, a.width)
     t_label = time.time() - t0
     xtr, ftr, ytr = features(train, rows_train)
+    # the last --val training states choose the epoch (lowest validation loss)
+    nfit = len(train) - a.val
     net = FloorProposerNet(max_batch=256, seed=0)
     t0 = time.time()
-    curve = net.train(xtr, ftr, ytr, epochs=a.epochs, batch=128, lr=2e-3, seed=0)
+    curve, val_curve = [], []
+    best = (float("inf"), -1, None)
+    for ep in range(a.epochs):
+        curve += net.train(xtr[:nfit], ftr[:nfit], ytr[:nfit], epochs=1, batch=128, lr=2e-3, seed=ep)
+        pv = net.forward(xtr[nfit:], ftr[nfit:]).double().cpu().numpy()
+        vl = float(-np.mean(np.log(np.maximum(pv[np.arange(a.val), ytr[nfit:]], 1e-30))))
+        val_curve.append(vl)
+        if vl < best[0]:
+            best = (vl, ep, net.get_params())
+    net.set_params(best[2])
     torch.cuda.synchronize()
     t_train = time.time() - t0
-    pred_tr = net.forward(xtr, ftr).argmax(1).cpu().numpy()
+    pred_tr = net.forward(xtr[:nfit], ftr[:nfit]).argmax(1).cpu().numpy()
+    pred_val = net.forward(xtr[nfit:], ftr[nfit:]).argmax(1).cpu().numpy()
 
     t0 = time.time()
-    plain_rows, learned_rows = evaluate(net, held)
+    rows = evaluate(net, held)
     t_eval = time.time() - t0
-    xho, fho, yho = features(held, plain_rows)
+    xho, fho, yho = features(held, rows["plain"])
     pred_ho = net.forward(xho, fho).argmax(1).cpu().numpy()
-    escalated = [r["predicted_raise_floor"] == 1 or r["n_floor_attempts"] > 1 for r in plain_rows]
+    escalated = [r["predicted_raise_floor"] == 1 or r["n_floor_attempts"] > 1 for r in rows["plain"]]
+
+    def confusion(y, p):
+        return np.histogram2d(y, p, bins=[3, 3], range=[[0, 3], [0, 3]])[0].astype(int).tolist()
+
     summary = {
-        "states": {"train": a.train, "heldout": a.heldout, "meshes": MESHES,
+        "states": {"train": nfit, "validation": a.val, "heldout": a.heldout, "meshes": MESHES,
                    "generator": {"filtered": {"void_p": [0.1, 0.6], "filter_r": [1.2, 2.5]},
                                  "unfiltered": {"void_p": [0.1, 0.8]}},
                    "simp_p": 3.0, "policy": dict(POLICY),
-                   "label_counts_train": np.bincount(ytr, minlength=3).tolist(),
+                   "label_counts_train": np.bincount(ytr[:nfit], minlength=3).tolist(),
+                   "label_counts_validation": np.bincount(ytr[nfit:], minlength=3).tolist(),
                    "label_counts_heldout": np.bincount(yho, minlength=3).tolist()},
         "seconds": {"generate_cpu": t_gen, "label_gpu": t_label, "train_gpu": t_train, "evaluate_gpu": t_eval},
-        "training": {"epochs": a.epochs, "batch": 128, "lr": 2e-3, "loss_curve": curve,
-                     "train_accuracy": float(np.mean(pred_tr == ytr)),
+        "training": {"epochs": a.epochs, "chosen_epoch": best[1], "batch": 128, "lr": 2e-3,
+                     "loss_curve": curve, "validation_loss_curve": val_curve,
+                     "train_accuracy": float(np.mean(pred_tr == ytr[:nfit])),
+                     "validation_accuracy": float(np.mean(pred_val == ytr[nfit:])),
                      "heldout_accuracy": float(np.mean(pred_ho == yho)),
-                     "heldout_confusion": np.histogram2d(yho, pred_ho, bins=[3, 3], range=[[0, 3], [0, 3]])[0]
-                     .astype(int).tolist()},
-        "heldout_plain_vs_learned": {
-            "all": compare(plain_rows, learned_rows),
-            "plain_escalated": compare(plain_rows, learned_rows, escalated),
-            "plain_kept": compare(plain_rows, learned_rows, [not e for e in escalated]),
-            "learned_stopped_at_r50": compare(plain_rows, learned_rows,
-                                              [bool(r["stopped_at_r50"]) for r in learned_rows]),
+                     "heldout_confusion": confusion(yho, pred_ho)},
+        "heldout_policies": {
+            "all": compare(rows),
+            "plain_escalated": compare(rows, escalated),
+            "plain_kept": compare(rows, [not e for e in escalated]),
         },
     }
     os.makedirs(a.out, exist_ok=True)

@@ -453,7 +453,7 @@ int simpfem_dense_cholesky_inverse(int n, double* A, double* Linv, int* info_hos
   if (n < 0 || (n > 0 && (!A || !Linv)) || !info_host)
     throw InvalidArg{"simpfem_dense_cholesky_inverse: bad argument"};
   DevBuf info;
-  info.alloc(sizeof(int));
+  info.alloc(2 * sizeof(int));
   SF_CUDA(dense_chol_inverse(A, n, Linv, info.as<int>(), S(stream)));
   SF_CUDA(cudaMemcpyAsync(info_host, info.p, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
   SF_CUDA(cudaStreamSynchronize(S(stream)));

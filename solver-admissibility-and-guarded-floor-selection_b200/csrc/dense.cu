@@ -22,8 +22,12 @@
 // Blocks of at most 32 rows are factored and inverted by one warp.  Every
 // other flop is an FP64 GEMM whose K range is cut to the non-zero part of a
 // triangular operand; the zero triangles are stored explicitly (Li starts
-// zeroed), so the cut is exact.  Total work n^3/3 for the factor plus n^3/3
-// for the inverse, as for potrf + trtri.
+// zeroed), so the cut is exact.  For a dense matrix the work is n^3/3 for the
+// factor plus n^3/3 for the inverse, as for potrf + trtri.  The coarsest
+// matrix of the hierarchy is banded (a 27-point stencil in lexicographic node
+// order: lower bandwidth ~3 (ny+1)(nz+1)); the band is measured from the data
+// and the GEMMs are cut to it (chol_inv_rec), which leaves about 2 n^2 bw flops,
+// nearly all of them in the fill-in of L^{-1}.
 #include "common.cuh"
 
 namespace simpfem {
@@ -45,6 +49,7 @@ struct DGemm {
   double alpha, beta;
   int tri;        // which operand is triangular (restricts the K range per tile)
   int lower_out;  // skip output tiles entirely above the diagonal
+  int tri_off = 0;  // TRI_OPB_LOWER: op(B)[k][j] is non-zero for k >= j + tri_off
 };
 
 // C = alpha * A op(B) + beta * C on the FP64 tensor cores (mma.sync m8n8k4):
@@ -89,7 +94,7 @@ __global__ void __launch_bounds__(GT) dgemm_kernel(DGemm g) {
   int kbeg = 0, kend = g.K;
   if (g.tri == TRI_OPA_LOWER) kend = min(kend, i0 + GM);
   if (g.tri == TRI_OPB_UPPER) kend = min(kend, j0 + GN);
-  if (g.tri == TRI_OPB_LOWER) kbeg = j0;
+  if (g.tri == TRI_OPB_LOWER) kbeg = max(0, j0 + g.tri_off);
   const int nk = kend > kbeg ? (kend - kbeg + GK - 1) / GK : 0;
   // copy mappings: "row-run" = one matrix row, 8 consecutive k; "k-run" = one
   // k row, 8 consecutive columns
@@ -254,7 +259,13 @@ __global__ void __launch_bounds__(32) chol_inv_leaf_kernel(const double* __restr
   }
 }
 
-cudaError_t chol_inv_rec(double* A, double* Li, int64_t n, int o, int m, int* info, cudaStream_t s) {
+// bw: lower bandwidth of A (A[i][j] == 0 for i - j > bw).  Band Cholesky
+// keeps L inside the band, so A21 and L21 are non-zero only in their top-right
+// R x (m1 - C0) corner (R = min(m2, bw), C0 = max(0, m1 - bw)) and the Schur
+// update touches only A22[0:R][0:R]; L^{-1} fills in, and its off-diagonal block
+// is -Li22[:, 0:R] * X[0:R, :] with X = L21 Li11 (R x m1).  With bw >= m - 1 this
+// is the dense algorithm; the skipped products are exact zeros.
+cudaError_t chol_inv_rec(double* A, double* Li, int64_t n, int o, int m, int bw, int* info, cudaStream_t s) {
   if (m <= 32) {
     chol_inv_leaf_kernel<<<1, 32, 0, s>>>(A, Li, n, o, m, info);
     return sf_launched(1);
@@ -262,26 +273,58 @@ cudaError_t chol_inv_rec(double* A, double* Li, int64_t n, int o, int m, int* in
   const int nb = (m + 31) / 32;
   const int m1 = 32 * ((nb + 1) / 2);
   const int m2 = m - m1;
-  cudaError_t e = chol_inv_rec(A, Li, n, o, m1, info, s);
+  const int R = std::min(m2, bw), C0 = std::max(0, m1 - bw), W = m1 - C0;
+  cudaError_t e = chol_inv_rec(A, Li, n, o, m1, bw, info, s);
   if (e != cudaSuccess) return e;
   double* A21 = A + (int64_t)(o + m1) * n + o;
   double* A22 = A + (int64_t)(o + m1) * n + o + m1;
   double* Li11 = Li + (int64_t)o * n + o;
   double* Li21 = Li + (int64_t)(o + m1) * n + o;
   double* Li22 = Li + (int64_t)(o + m1) * n + o + m1;
-  // Li21 <- A21 * Li11^T  (op(B) = Li11^T is upper triangular)
-  e = dgemm(DGemm{m2, m1, m1, A21, n, Li11, n, Li21, n, 1.0, 0.0, TRI_OPB_UPPER, 0}, 1, s);
+  if (R > 0) {
+    // L21[0:R, C0:m1] <- A21[0:R, C0:m1] * Li11[C0:m1, C0:m1]^T  (op(B) upper triangular)
+    e = dgemm(DGemm{R, W, W, A21 + C0, n, Li11 + (int64_t)C0 * n + C0, n, Li21 + C0, n, 1.0, 0.0, TRI_OPB_UPPER,
+                    0},
+              1, s);
+    if (e != cudaSuccess) return e;
+    // A22[0:R, 0:R] <- A22 - L21 L21^T  (lower tiles)
+    e = dgemm(DGemm{R, R, W, Li21 + C0, n, Li21 + C0, n, A22, n, -1.0, 1.0, TRI_NONE, 1}, 1, s);
+    if (e != cudaSuccess) return e;
+  }
+  e = chol_inv_rec(A, Li, n, o + m1, m2, bw, info, s);
   if (e != cudaSuccess) return e;
-  // A22 <- A22 - Li21 * Li21^T  (lower tiles)
-  e = dgemm(DGemm{m2, m2, m1, Li21, n, Li21, n, A22, n, -1.0, 1.0, TRI_NONE, 1}, 1, s);
-  if (e != cudaSuccess) return e;
-  e = chol_inv_rec(A, Li, n, o + m1, m2, info, s);
-  if (e != cudaSuccess) return e;
-  // A21 <- Li21 * Li11  (Li11 lower triangular)
-  e = dgemm(DGemm{m2, m1, m1, Li21, n, Li11, n, A21, n, 1.0, 0.0, TRI_OPB_LOWER, 0}, 0, s);
-  if (e != cudaSuccess) return e;
-  // Li21 <- -Li22 * A21  (Li22 lower triangular)
-  return dgemm(DGemm{m2, m1, m2, Li22, n, A21, n, Li21, n, -1.0, 0.0, TRI_OPA_LOWER, 0}, 0, s);
+  if (R == 0) return cudaSuccess;  // L21 = 0: the off-diagonal block of L^{-1} stays zero
+  // X = A21[0:R, 0:m1] <- L21[0:R, C0:m1] * Li11[C0:m1, 0:m1]  (Li11 lower: row C0 + k is non-zero for
+  // columns j <= C0 + k)
+  {
+    DGemm g{R, m1, W, Li21 + C0, n, Li11 + (int64_t)C0 * n, n, A21, n, 1.0, 0.0, TRI_OPB_LOWER, 0};
+    g.tri_off = -C0;
+    e = dgemm(g, 0, s);
+    if (e != cudaSuccess) return e;
+  }
+  // Li21 <- -Li22[:, 0:R] * X[0:R, :]  (Li22 lower triangular)
+  return dgemm(DGemm{m2, m1, R, Li22, n, A21, n, Li21, n, -1.0, 0.0, TRI_OPA_LOWER, 0}, 0, s);
+}
+
+// lower bandwidth of a row-major n x n matrix: max over rows of i - (first
+// column j <= i with A[i][j] != 0; NaN counts as non-zero); one warp per row
+__global__ void lower_band_kernel(const double* __restrict__ A, int n, int* __restrict__ bw) {
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = (int)warp;
+  const double* row = A + (int64_t)i * n;
+  int first = i;
+  for (int j0 = 0; j0 <= i; j0 += 32) {
+    const int j = j0 + lane;
+    const bool nz = j <= i && row[j] != 0.0;
+    const unsigned b = __ballot_sync(0xffffffffu, nz);
+    if (b) {
+      first = j0 + __ffs((int)b) - 1;
+      break;
+    }
+  }
+  if (lane == 0 && i - first > 0) atomicMax(bw, i - first);
 }
 
 __global__ void transpose_kernel(const double* __restrict__ A, int n, double* __restrict__ At) {
@@ -314,7 +357,18 @@ cudaError_t dense_chol_inverse(double* A, int n, double* Linv, int* info_dev, cu
   e = cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, s);
   if (e != cudaSuccess) return e;
   if (n <= 0) return cudaSuccess;
-  e = chol_inv_rec(A, Linv, n, 0, n, info_dev, s);
+  // the band (exact zeros below it) decides which blocks the recursion multiplies
+  e = cudaMemsetAsync(info_dev + 1, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  lower_band_kernel<<<div_up((int64_t)n * 32, 256), 256, 0, s>>>(A, n, info_dev + 1);
+  e = sf_launched(1);
+  if (e != cudaSuccess) return e;
+  int bw = 0;
+  e = cudaMemcpyAsync(&bw, info_dev + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  e = chol_inv_rec(A, Linv, n, 0, n, std::max(bw, 0), info_dev, s);
   if (e != cudaSuccess) return e;
   const int64_t nn = (int64_t)n * n;
   nonfinite_flag_kernel<<<(int)std::min<int64_t>(div_up(nn, 256), 148 * 16), 256, 0, s>>>(Linv, nn, n + 1,

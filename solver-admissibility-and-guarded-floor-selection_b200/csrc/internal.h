@@ -181,8 +181,10 @@ cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloo
                               cudaStream_t s);
 
 // Linv <- L^{-1} (lower, zero upper) of the Cholesky factor of the SPD row-major
-// A (destroyed).  *info_dev: 0, or the 1-based index of the first non-positive
-// pivot, or n + 1 when L^{-1} holds a non-finite entry.
+// A (destroyed).  info_dev[0]: 0, or the 1-based index of the first non-positive
+// pivot, or n + 1 when L^{-1} holds a non-finite entry; info_dev[1] is scratch
+// (the measured lower bandwidth of A, which decides the blocks multiplied).
+// Synchronises the stream once (the bandwidth is read on the host).
 cudaError_t dense_chol_inverse(double* A, int n, double* Linv, int* info_dev, cudaStream_t s);
 cudaError_t launch_transpose(const double* A, int n, double* At, cudaStream_t s);
 cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b,

@@ -1,14 +1,15 @@
 """Standalone launches of single kernels of the library, for timing and for ncu.
 
     python profile_kernels.py smoother-step NX NY NZ [REPS] [--stack plain|canonical] [--precision fp32|fp64]
-    python profile_kernels.py dense N [REPS]
+    python profile_kernels.py dense N [REPS] [--band BW]
 
 smoother-step: builds the 4-level hierarchy on an NX x NY x NZ cantilever
 (random E in [1e-3, 1.001)), then times REPS fused fine smoothing steps with
 simpfem_gmg_time_smoother_step (each launch after an L2-evicting write, on
 pseudo-random vectors) and prints the average launch time and the algorithmic
-bandwidth.  dense: factors and inverts a random SPD N x N matrix with
-simpfem_dense_cholesky_inverse REPS times and prints the best time and FP64 rate.
+bandwidth.  dense: factors and inverts a random SPD N x N matrix (banded with
+lower bandwidth BW when --band is given, as the coarsest level is) with
+simpfem_dense_cholesky_inverse REPS times and prints the best time.
 Both exit 0 on success, so the same command line can run under ncu afterwards.
 """
 
@@ -59,8 +60,17 @@ def dense(a) -> None:
     n = a.n
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
-    Q = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
-    A0 = Q @ Q.T / n + torch.eye(n, dtype=torch.float64, device="cuda")
+    if a.band is None:
+        Q = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+        A0 = Q @ Q.T / n + torch.eye(n, dtype=torch.float64, device="cuda")
+    else:
+        # symmetric, band of random entries, diagonally dominant
+        R = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+        i = torch.arange(n, device="cuda")
+        inband = (i[:, None] - i[None, :]).abs() <= a.band
+        A0 = torch.where(inband, R, torch.zeros_like(R))
+        A0 = torch.tril(A0, -1) + torch.tril(A0, -1).T + torch.diag(torch.full((n,), 2.0 * a.band + 2.0,
+                                                                             dtype=torch.float64, device="cuda"))
     A = torch.empty_like(A0)
     Li = torch.empty_like(A0)
     info = ctypes.c_int()
@@ -77,8 +87,11 @@ def dense(a) -> None:
         best = min(best, e0.elapsed_time(e1))
     if info.value != 0:
         raise SystemExit(f"factorisation failed: info {info.value}")
-    gflop = 2.0 * n ** 3 / 3.0 / 1e9
-    print(f"dense n={n}: best {best:.3f} ms over {a.reps}, {gflop:.1f} GFLOP, {gflop / best:.2f} TFLOP/s")
+    if a.band is None:
+        gflop = 2.0 * n ** 3 / 3.0 / 1e9
+        print(f"dense n={n}: best {best:.3f} ms over {a.reps}, {gflop:.1f} GFLOP, {gflop / best:.2f} TFLOP/s")
+    else:
+        print(f"dense n={n} band={a.band}: best {best:.3f} ms over {a.reps}")
 
 
 def main() -> None:
@@ -94,6 +107,7 @@ def main() -> None:
     d = sub.add_parser("dense")
     d.add_argument("n", type=int)
     d.add_argument("reps", type=int, nargs="?", default=5)
+    d.add_argument("--band", type=int, default=None)
     a = ap.parse_args()
     smoother_step(a) if a.cmd == "smoother-step" else dense(a)
 

@@ -73,3 +73,42 @@ def test_non_finite_input_fails(cuda):
     A[70, 3] = A[3, 70] = np.nan
     _, info = _factor(cuda, A)
     assert info != 0
+
+
+def _banded_spd(n, bw, seed, scales=None):
+    rng = np.random.default_rng(seed)
+    A = np.zeros((n, n))
+    for d in range(1, bw + 1):
+        v = rng.standard_normal(n - d)
+        A[np.arange(d, n), np.arange(n - d)] = v
+        A[np.arange(n - d), np.arange(d, n)] = v
+    A[np.arange(n), np.arange(n)] = 2.0 * bw + 1.0 + rng.uniform(0.0, 1.0, n)  # diagonally dominant
+    if scales is not None:
+        A *= np.sqrt(np.outer(scales, scales))
+    return A
+
+
+@pytest.mark.parametrize("n,bw", [(300, 1), (500, 37), (1000, 219), (1000, 999), (3960, 219), (2049, 64)])
+def test_banded_inverse_factor_matches_numpy(cuda, n, bw):
+    """The coarsest matrix is banded; the recursion multiplies only the band's
+    non-zero blocks, measured from the data (bw = n - 1 is the dense case)."""
+    A = _banded_spd(n, bw, n + bw)
+    Li, info = _factor(cuda, A)
+    ref = np.linalg.inv(np.linalg.cholesky(A))
+    assert info == 0
+    assert np.abs(Li - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.all(np.triu(Li, 1) == 0.0)
+
+
+def test_banded_with_one_wide_row_and_scales(cuda):
+    # one entry far below the band widens the measured band to that row's reach;
+    # SIMP-like scales (1e-9 .. 1) as on a coarse level with void regions
+    n, bw = 1500, 40
+    rng = np.random.default_rng(5)
+    A = _banded_spd(n, bw, 6, scales=10.0 ** rng.uniform(-9, 0, n))
+    A[1200, 100] = A[100, 1200] = 0.5 * np.sqrt(A[1200, 1200] * A[100, 100])
+    b = rng.standard_normal(n)
+    Li, info = _factor(cuda, A)
+    assert info == 0
+    x = Li.T @ (Li @ b)
+    assert np.linalg.norm(A @ x - b) <= 1e-8 * np.linalg.norm(b)

@@ -413,8 +413,10 @@ static void level_op(Gmg& G, int l, DType vt, int precsel, Epi epi, const void* 
   const void* coef = L.K64.p;
   if (vt == F32) {
     if (precsel == BF16 && L.K16.p) {
-      ct = BF16;
-      coef = L.K16.p;
+      // BF16 copy node-major by neighbour column, nine lanes per node
+      SF_CUDA(launch_stencil_col_bf16(epi, L.g, L.K16.as<__nv_bfloat16>(), L.mask.as<uint8_t>(), (const float*)u,
+                                      ea, G.st));
+      return;
     } else {
       ct = F32;
       coef = L.K32.p;
@@ -1243,8 +1245,8 @@ void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
       }
     }
     if (G.cyc == F32 && p == BF16) {
-      L.K16.alloc(2 * 243 * L.g.nn);
-      SF_CUDA(launch_convert(F64, BF16, L.K64.p, L.K16.p, 243 * L.g.nn, nullptr, G.st));
+      L.K16.alloc(2 * 288 * L.g.nn);  // node-major by neighbour column, 288 entries per node
+      SF_CUDA(launch_stencil_colmajor_bf16(L.g.nn, L.K64.as<double>(), L.K16.as<__nv_bfloat16>(), G.st));
     }
   }
   pt.mark("precision copies");

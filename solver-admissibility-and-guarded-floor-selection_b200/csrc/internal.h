@@ -126,6 +126,12 @@ cudaError_t launch_element_energy(const Grid& g, const double* u_full, double* c
 // ------------------------------------------------------------- stencil.cu
 // Coarse operators: 27-point 3x3-block stencils, coefficient c(o, r, q) of node n
 // stored at coef[(o * 9 + r * 3 + q) * nn + n] (o = (dx+1)*9 + (dy+1)*3 + (dz+1)).
+// BF16 copy of an FP64 structure-of-arrays stencil operator, node-major by
+// neighbour column (288 entries per node), and the stencil application on it
+// (FP32 vectors, nine lanes per node) used by the mixed cycle.
+cudaError_t launch_stencil_colmajor_bf16(int64_t nn, const double* K64, __nv_bfloat16* out, cudaStream_t s);
+cudaError_t launch_stencil_col_bf16(Epi epi, const Grid& g, const __nv_bfloat16* coefC, const uint8_t* mask,
+                                    const float* u, const EpiArgs& ea, cudaStream_t s);
 cudaError_t launch_stencil(DType vt, DType ct, Epi epi, const Grid& g, const void* coef,
                            const uint8_t* mask, const void* u, const EpiArgs& ea, cudaStream_t s);
 cudaError_t launch_level1_assemble(const Grid& gc, const Grid& gf, const double* E_fine,

@@ -82,7 +82,21 @@ __global__ void __launch_bounds__(kRedThreads) dots_kernel(int64_t n, DotSet ds,
 #pragma unroll
   for (int k = 0; k < ND; ++k) v[k] = 0.0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // four strided elements per pass: their loads are independent and in flight
+  // together (one load per vector per thread left the kernel latency-bound)
+  for (; i + 3 * stride < n; i += 4 * stride) {
+#pragma unroll
+    for (int k = 0; k < ND; ++k) {
+      const double t0 = dot_term<T>(ds, k, i), t1 = dot_term<T>(ds, k, i + stride);
+      const double t2 = dot_term<T>(ds, k, i + 2 * stride), t3 = dot_term<T>(ds, k, i + 3 * stride);
+      v[k] += t0;
+      v[k] += t1;
+      v[k] += t2;
+      v[k] += t3;
+    }
+  }
+  for (; i < n; i += stride) {
 #pragma unroll
     for (int k = 0; k < ND; ++k) v[k] += dot_term<T>(ds, k, i);
   }
@@ -529,7 +543,24 @@ __global__ void __launch_bounds__(kRedThreads) mgs_step_kernel(int64_t n, const 
   const double h = *hi;
   double v[1] = {0.0};
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // four strided elements per pass (independent loads in flight together)
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    double wv[4], vv[4], nv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      wv[q] = w[i + q * stride];
+      vv[q] = vi[i + q * stride];
+      if (vnext != nullptr) nv[q] = vnext[i + q * stride];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double wn = sub_rn(wv[q], mul_rn(h, vv[q]));
+      w[i + q * stride] = wn;
+      v[0] += (vnext != nullptr ? nv[q] : wn) * wn;
+    }
+  }
+  for (; i < n; i += stride) {
     const double wn = sub_rn(w[i], mul_rn(h, vi[i]));
     w[i] = wn;
     v[0] += (vnext != nullptr ? vnext[i] : wn) * wn;

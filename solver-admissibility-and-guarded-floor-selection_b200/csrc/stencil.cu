@@ -98,6 +98,142 @@ cudaError_t launch_stencil(DType vt, DType ct, Epi epi, const Grid& g, const voi
 }
 
 // ----------------------------------------------------------------------------
+// BF16 stencils of the mixed-precision cycle, node-major by neighbour column:
+// coefC[n * 288 + col * 32 + oz * 9 + r * 3 + q] with col = ox * 3 + oy, i.e.
+// the 27 coefficients coupling node n to its three z-neighbours in column
+// (ox, oy) in one 64-byte slot (entries 27..31 zero).  Made from the FP64
+// structure-of-arrays operator once per setup.
+//
+// Nine lanes per node, three nodes per warp: lane (t, col) loads its slot with
+// four 16-byte loads and the 9 vector entries of its z-neighbours, forms its
+// part of the node's three row sums, and the node's first lane adds the nine
+// parts (in column order, through shared memory) and applies the epilogue with
+// operands it read up front.  The row-per-thread kernel above chains 81 loads
+// per thread (latency-bound on the small coarse levels) and a warp per node
+// spends its issue slots on per-node index and reduction work; this split keeps
+// both small.
+constexpr int kColSlot = 32, kNodeStrideC = 9 * kColSlot;
+
+// 32 nodes per block: coalesced reads along n of the FP64 operator, the tile
+// transposed through shared memory, coalesced node-major BF16 writes
+__global__ void __launch_bounds__(256) stencil_colmajor_bf16_kernel(int nn, const double* __restrict__ K64,
+                                                                     __nv_bfloat16* __restrict__ out) {
+  __shared__ __nv_bfloat16 tile[32 * kNodeStrideC];
+  const int n0 = blockIdx.x * 32;
+  const int nl = threadIdx.x & 31, c0 = threadIdx.x >> 5;
+  const int cnt = min(32, nn - n0);
+  for (int c = c0; c < kNodeStrideC; c += 8) {
+    const int col = c / kColSlot, w = c % kColSlot;
+    float v = 0.f;
+    if (nl < cnt && w < 27) {
+      const int o = col * 3 + w / 9;  // o = ox * 9 + oy * 3 + oz
+      v = (float)K64[(int64_t)(o * 9 + w % 9) * nn + n0 + nl];
+    }
+    tile[nl * kNodeStrideC + c] = __float2bfloat16_rn(v);
+  }
+  __syncthreads();
+  __nv_bfloat16* dst = out + (int64_t)n0 * kNodeStrideC;
+  for (int e = threadIdx.x; e < cnt * kNodeStrideC; e += blockDim.x) dst[e] = tile[e];
+}
+
+cudaError_t launch_stencil_colmajor_bf16(int64_t nn, const double* K64, __nv_bfloat16* out, cudaStream_t s) {
+  if (nn <= 0) return cudaSuccess;
+  if (nn * kNodeStrideC >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
+  stencil_colmajor_bf16_kernel<<<div_up(nn, 32), 256, 0, s>>>((int)nn, K64, out);
+  return sf_launched(1);
+}
+
+__device__ __forceinline__ float bf16_lo(unsigned w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
+
+template <int EPI>
+__global__ void __launch_bounds__(256) stencil_col_bf16_kernel(Grid g, const __nv_bfloat16* __restrict__ coefC,
+                                                               const uint8_t* __restrict__ mask,
+                                                               const float* __restrict__ u, EpiArgs ea) {
+  __shared__ float part[8][27][3];
+  if (guard_off(ea.guard)) return;
+  const int nn = (int)g.nn;
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (warp * 3 >= nn) return;  // whole warps leave together
+  const int t = lane / 9, col = lane - 9 * t;
+  const int64_t n64 = warp * 3 + t;
+  const bool act = lane < 27 && n64 < nn;
+  const int n = act ? (int)n64 : 0;
+  EpiOperands<float, EPI> eo;
+  float xv[3];
+  if (act && col == 0) {
+    eo.load(ea, 3 * (int64_t)n, mask);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) xv[c] = u[3 * n + c];
+  }
+  float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+  if (act) {
+    const int NZ1 = g.nz + 1, NY1 = g.ny + 1;
+    const int k = n % NZ1, jq = n / NZ1;
+    const int j = jq % NY1, i = jq / NY1;
+    const int ox = col / 3, oy = col % 3;
+    // a neighbour outside the grid has zero coefficients: clamp it to the node itself
+    const int dx = (ox == 0) ? (i > 0 ? -NY1 * NZ1 : 0) : (ox == 2 ? (i < g.nx ? NY1 * NZ1 : 0) : 0);
+    const int dy = (oy == 0) ? (j > 0 ? -NZ1 : 0) : (oy == 2 ? (j < g.ny ? NZ1 : 0) : 0);
+    const int base = n + dx + dy;
+    const uint4* cp = reinterpret_cast<const uint4*>(coefC + (int64_t)n * kNodeStrideC + col * kColSlot);
+    const uint4 q0 = cp[0], q1 = cp[1], q2 = cp[2], q3 = cp[3];
+    const unsigned wv[16] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w,
+                             q2.x, q2.y, q2.z, q2.w, q3.x, q3.y, q3.z, q3.w};
+    float cf[28];
+#pragma unroll
+    for (int e = 0; e < 14; ++e) {
+      cf[2 * e] = bf16_lo(wv[e]);
+      cf[2 * e + 1] = bf16_hi(wv[e]);
+    }
+#pragma unroll
+    for (int oz = 0; oz < 3; ++oz) {
+      const int dz = (oz == 0) ? (k > 0 ? -1 : 0) : (oz == 2 ? (k < g.nz ? 1 : 0) : 0);
+      const float* um = u + 3 * (base + dz);
+      const float u0 = um[0], u1 = um[1], u2 = um[2];
+      const float* c = cf + oz * 9;
+      p0 = fmaf(c[0], u0, fmaf(c[1], u1, fmaf(c[2], u2, p0)));
+      p1 = fmaf(c[3], u0, fmaf(c[4], u1, fmaf(c[5], u2, p1)));
+      p2 = fmaf(c[6], u0, fmaf(c[7], u1, fmaf(c[8], u2, p2)));
+    }
+  }
+  if (lane < 27) {
+    part[wib][lane][0] = p0;
+    part[wib][lane][1] = p1;
+    part[wib][lane][2] = p2;
+  }
+  __syncwarp();
+  if (act && col == 0) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+    for (int cc = 0; cc < 9; ++cc) {
+      a0 += part[wib][lane + cc][0];
+      a1 += part[wib][lane + cc][1];
+      a2 += part[wib][lane + cc][2];
+    }
+    eo.apply(ea, 3 * (int64_t)n, 0, a0, xv[0]);
+    eo.apply(ea, 3 * (int64_t)n + 1, 1, a1, xv[1]);
+    eo.apply(ea, 3 * (int64_t)n + 2, 2, a2, xv[2]);
+  }
+}
+
+cudaError_t launch_stencil_col_bf16(Epi epi, const Grid& g, const __nv_bfloat16* coefC, const uint8_t* mask,
+                                    const float* u, const EpiArgs& ea, cudaStream_t s) {
+  if (3 * g.nn >= (int64_t(1) << 31) || g.nn * kNodeStrideC >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
+  const int nb = div_up(div_up(g.nn, 3), 8);
+  switch (epi) {
+    case EPI_APPLY: stencil_col_bf16_kernel<EPI_APPLY><<<nb, 256, 0, s>>>(g, coefC, mask, u, ea); break;
+    case EPI_RESID: stencil_col_bf16_kernel<EPI_RESID><<<nb, 256, 0, s>>>(g, coefC, mask, u, ea); break;
+    case EPI_CHEB1: stencil_col_bf16_kernel<EPI_CHEB1><<<nb, 256, 0, s>>>(g, coefC, mask, u, ea); break;
+    case EPI_CHEB: stencil_col_bf16_kernel<EPI_CHEB><<<nb, 256, 0, s>>>(g, coefC, mask, u, ea); break;
+    case EPI_JAC: stencil_col_bf16_kernel<EPI_JAC><<<nb, 256, 0, s>>>(g, coefC, mask, u, ea); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return sf_launched(1);
+}
+
+// ----------------------------------------------------------------------------
 // Level-1 Galerkin operator from the fine element moduli: for every coarse
 // element C and sub-element stu, E_fine[child(C, stu)] * Q_stu with
 // Q_stu = P24(stu)^T KE P24(stu), child clamped to the fine grid exactly as

@@ -222,7 +222,7 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
     for (int nt : {128, 256, maxt}) {
       const int bj = nt / bk;
       if (bj < 2 || bj * bk > maxt) continue;
-      for (int cx : {4, 8, 16}) {
+      for (int cx : {4, 6, 8, 10, 12, 14, 16, 20}) {  // fine steps: the wave count depends on it
         SweepShape sh;
         sh.bj = bj;
         sh.bk = bk;

@@ -307,6 +307,42 @@ __device__ __forceinline__ double w1(const double* w, int f, int c) {
 }
 
 // K_c = R K_f P on stencils (Galerkin triple product of the reference's RAP loop).
+// Coarse block (n, M = n + o) = sum over fine nodes f in the support of n and
+// fine neighbours g = f + d of f in the support of M of
+// P[f, n] K_f[f, g] P[g, M].  The trilinear weights factor per axis, so each
+// axis contributes a list of at most 7 valid (f, d) pairs with weight
+// w(f, I) w(g, I + m) (m the axis component of o), and the sum runs over the
+// product of the three lists: only non-zero terms, no per-term bounds checks
+// or weight lookups (the thread is otherwise bound by that scan of 27 x 27
+// candidate pairs).
+struct RapAxis {
+  double w[7];
+  int64_t off[7];  // fine-node offset (f - 2I) * node stride + d * stencil-block stride
+  int cnt;
+};
+
+__device__ __forceinline__ void rap_axis(RapAxis& ax, const double* __restrict__ w, int I, int m, int nf,
+                                         int64_t node_stride, int64_t blk_stride) {
+  ax.cnt = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int f = 2 * I + a - 1;
+    if (f < 0 || f > nf) continue;
+    const double wf = w1(w, f, I);
+    if (wf == 0.0) continue;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int gg = f + d - 1;
+      if (gg < 0 || gg > nf) continue;
+      const double wg = w1(w, gg, I + m);
+      if (wg == 0.0) continue;
+      ax.w[ax.cnt] = wf * wg;
+      ax.off[ax.cnt] = (int64_t)(a - 1) * node_stride + (int64_t)d * blk_stride;
+      ++ax.cnt;
+    }
+  }
+}
+
 __global__ void rap_kernel(Grid gf, Grid gc, const double* __restrict__ cf, const uint8_t* __restrict__ mask_c,
                            const double* __restrict__ wx, const double* __restrict__ wy,
                            const double* __restrict__ wz, double* __restrict__ cc) {
@@ -316,27 +352,34 @@ __global__ void rap_kernel(Grid gf, Grid gc, const double* __restrict__ cf, cons
   const int64_t n = idx - (int64_t)o * gc.nn;
   int I, J, K;
   node_ijk(gc, n, I, J, K);
-  const int MI = I + o / 9 - 1, MJ = J + (o / 3) % 3 - 1, MK = K + o % 3 - 1;
+  const int mx = o / 9 - 1, my = (o / 3) % 3 - 1, mz = o % 3 - 1;
+  const int MI = I + mx, MJ = J + my, MK = K + mz;
   double blk[9];
 #pragma unroll
   for (int r = 0; r < 9; ++r) blk[r] = 0.0;
   const bool nb_ok = MI >= 0 && MJ >= 0 && MK >= 0 && MI <= gc.nx && MJ <= gc.ny && MK <= gc.nz;
   if (nb_ok) {
-    for (int d1 = 0; d1 < 27; ++d1) {
-      const int fi = 2 * I + d1 / 9 - 1, fj = 2 * J + (d1 / 3) % 3 - 1, fk = 2 * K + d1 % 3 - 1;
-      if (fi < 0 || fj < 0 || fk < 0 || fi > gf.nx || fj > gf.ny || fk > gf.nz) continue;
-      const double p1 = w1(wx, fi, I) * w1(wy, fj, J) * w1(wz, fk, K);
-      if (p1 == 0.0) continue;
-      const int64_t f1 = node_id(gf, fi, fj, fk);
-      for (int of = 0; of < 27; ++of) {
-        const int gi = fi + of / 9 - 1, gj = fj + (of / 3) % 3 - 1, gk = fk + of % 3 - 1;
-        if (gi < 0 || gj < 0 || gk < 0 || gi > gf.nx || gj > gf.ny || gk > gf.nz) continue;
-        const double p2 = w1(wx, gi, MI) * w1(wy, gj, MJ) * w1(wz, gk, MK);
-        if (p2 == 0.0) continue;
-        const double pp = p1 * p2;
-        const double* src = cf + (int64_t)of * 9 * gf.nn + f1;
+    const int64_t nn = gf.nn, NZ1 = gf.nz + 1, NY1 = gf.ny + 1;
+    // stencil block of offset (dx, dy, dz) starts at ((dx * 9 + dy * 3 + dz) * 9) * nn
+    RapAxis ax, ay, az;
+    rap_axis(ax, wx, I, mx, gf.nx, NY1 * NZ1, 81 * nn);
+    rap_axis(ay, wy, J, my, gf.ny, NZ1, 27 * nn);
+    rap_axis(az, wz, K, mz, gf.nz, 1, 9 * nn);
+    // index of the fine node (2I, 2J, 2K); every listed pair adds an offset that
+    // lands on a fine node inside the grid
+    const int64_t base = node_id(gf, 2 * I, 2 * J, 2 * K);
+    for (int ex = 0; ex < ax.cnt; ++ex) {
+      for (int ey = 0; ey < ay.cnt; ++ey) {
+        const double wxy = ax.w[ex] * ay.w[ey];
+        const int64_t bxy = base + ax.off[ex] + ay.off[ey];
 #pragma unroll
-        for (int r = 0; r < 9; ++r) blk[r] += pp * src[(int64_t)r * gf.nn];
+        for (int ez = 0; ez < 7; ++ez) {
+          if (ez >= az.cnt) break;
+          const double pp = wxy * az.w[ez];
+          const double* src = cf + (bxy + az.off[ez]);
+#pragma unroll
+          for (int r = 0; r < 9; ++r) blk[r] += pp * src[(int64_t)r * nn];
+        }
       }
     }
   }

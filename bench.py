@@ -236,12 +236,15 @@ def run_native(args):
         # host_io: pinned host densities in, each solution x back to the host, inside the timed region
         if host_io:
             dens = [torch.as_tensor(states[s]).pin_memory() for s in seq]
+            # pinned result buffers; each solution is copied asynchronously on its
+            # worker's stream (the stream order keeps it ahead of the next solve)
+            xs = [torch.empty(bp.workers[0].F_free_gpu.numel(), dtype=torch.float64).pin_memory() for _ in seq]
         else:
             dens = [torch.as_tensor(states[s], device="cuda") for s in seq]
-        xs = {}
+            xs = []
 
         def keep_x(k, worker, row):
-            xs[k] = worker.last_x.to("cpu")
+            xs[k].copy_(worker.last_x, non_blocking=True)
 
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

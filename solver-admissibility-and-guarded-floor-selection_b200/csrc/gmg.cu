@@ -590,8 +590,12 @@ static void solve_coarsest(Gmg& G, const void* rhs, void* x) {
   }
   if (G.coarse_mode == 1) {
     SF_CUDA(launch_gather_idx(G.nc, G.c_idx.as<int32_t>(), b64, G.cb.as<double>(), G.guard, G.st));
-    SF_CUDA(launch_coarsest_solve(G.Linv.as<double>(), G.LinvT.as<double>(), G.nc, G.cb.as<double>(),
-                                  G.ctmp.as<double>(), G.cx.as<double>(), G.guard, G.st));
+    if (G.cyc == F32 && G.LinvF.p)
+      SF_CUDA(launch_coarsest_solve_f32(G.LinvF.as<float>(), G.LinvTF.as<float>(), G.nc, G.cb.as<double>(),
+                                        G.ctmp.as<double>(), G.cx.as<double>(), G.guard, G.st));
+    else
+      SF_CUDA(launch_coarsest_solve(G.Linv.as<double>(), G.LinvT.as<double>(), G.nc, G.cb.as<double>(),
+                                    G.ctmp.as<double>(), G.cx.as<double>(), G.guard, G.st));
     SF_CUDA(launch_fill(F64, n, 0.0, x64, G.guard, G.st));
     SF_CUDA(launch_scatter_idx(G.nc, G.c_idx.as<int32_t>(), G.cx.as<double>(), x64, G.guard, G.st));
   } else {
@@ -1128,6 +1132,14 @@ static void setup_coarsest(Gmg& G) {
     if (ok) {
       G.LinvT.alloc(8 * (size_t)n * n);
       SF_CUDA(launch_transpose(G.Linv.as<double>(), n, G.LinvT.as<double>(), G.st));
+      if (G.cyc == F32) {
+        // the mixed cycle reads FP32 copies of both factors (FP64 accumulation)
+        const int64_t nn2 = (int64_t)n * n;
+        G.LinvF.alloc(4 * (size_t)nn2);
+        G.LinvTF.alloc(4 * (size_t)nn2);
+        SF_CUDA(launch_convert(F64, F32, G.Linv.p, G.LinvF.p, nn2, nullptr, G.st));
+        SF_CUDA(launch_convert(F64, F32, G.LinvT.p, G.LinvTF.p, nn2, nullptr, G.st));
+      }
       G.coarse_mode = 1;
       return;
     }

@@ -188,6 +188,7 @@ struct Gmg {
   bool coarse_reg = false;
   int nc = 0;
   DevBuf c_idx, c_didx, Adense, Linv, LinvT, cb, cx, ctmp, cinfo;
+  DevBuf LinvF, LinvTF;  // FP32 copies of Linv and LinvT read by the mixed cycle
   // iterative coarse (fixed PCG) vectors
   DevBuf pr, pz, pp, pAp;
 

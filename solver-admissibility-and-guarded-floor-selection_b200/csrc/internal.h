@@ -195,6 +195,9 @@ cudaError_t dense_chol_inverse(double* A, int n, double* Linv, int* info_dev, cu
 cudaError_t launch_transpose(const double* A, int n, double* At, cudaStream_t s);
 cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b,
                                   double* tmp, double* x, const int* guard, cudaStream_t s);
+// the same with FP32 copies of L^{-1} and L^{-T} (FP64 vectors and accumulation)
+cudaError_t launch_coarsest_solve_f32(const float* Linv, const float* LinvT, int n, const double* b,
+                                      double* tmp, double* x, const int* guard, cudaStream_t s);
 cudaError_t launch_add_diag(double* A, int n, double eps, cudaStream_t s);
 cudaError_t launch_diag_sum(const double* A, int n, double* out, cudaStream_t s);
 cudaError_t launch_all_finite(const double* A, int64_t n, int* flag, cudaStream_t s);

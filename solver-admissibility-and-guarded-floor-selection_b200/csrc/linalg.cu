@@ -458,17 +458,28 @@ cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloo
 
 // y = M b over the triangle of a dense row-major M (lower: j <= i, upper: j >= i),
 // one warp per row.
-template <int UPPER>
-__global__ void tri_matvec_kernel(const double* __restrict__ M, int n, const double* __restrict__ b,
+// y = L b (UPPER = 0: lower rows 0..row) or L^T b stored transposed (UPPER = 1),
+// one warp per row, FP64 accumulation; the matrix may be stored in FP32 (the
+// mixed cycle's copy).  Four strided loads per lane are in flight per pass.
+template <int UPPER, typename MT>
+__global__ void tri_matvec_kernel(const MT* __restrict__ M, int n, const double* __restrict__ b,
                                   double* __restrict__ y, const int* guard) {
   if (guard_off(guard)) return;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= n) return;
-  const double* r = M + (int64_t)row * n;
+  const MT* r = M + (int64_t)row * n;
   const int lo = UPPER ? row : 0, hi = UPPER ? n : row + 1;
-  double s = 0.0;
-  for (int j = lo + lane; j < hi; j += 32) s += r[j] * b[j];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int j = lo + lane;
+  for (; j + 96 < hi; j += 128) {
+    s0 += (double)r[j] * b[j];
+    s1 += (double)r[j + 32] * b[j + 32];
+    s2 += (double)r[j + 64] * b[j + 64];
+    s3 += (double)r[j + 96] * b[j + 96];
+  }
+  for (; j < hi; j += 32) s0 += (double)r[j] * b[j];
+  double s = (s0 + s1) + (s2 + s3);
   s = warp_sum(s);
   if (lane == 0) y[row] = s;
 }
@@ -476,8 +487,16 @@ __global__ void tri_matvec_kernel(const double* __restrict__ M, int n, const dou
 cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b, double* tmp,
                                   double* x, const int* guard, cudaStream_t s) {
   const int blocks = div_up((int64_t)n * 32, 256);
-  tri_matvec_kernel<0><<<blocks, 256, 0, s>>>(Linv, n, b, tmp, guard);
-  tri_matvec_kernel<1><<<blocks, 256, 0, s>>>(LinvT, n, tmp, x, guard);
+  tri_matvec_kernel<0, double><<<blocks, 256, 0, s>>>(Linv, n, b, tmp, guard);
+  tri_matvec_kernel<1, double><<<blocks, 256, 0, s>>>(LinvT, n, tmp, x, guard);
+  return sf_launched(2);
+}
+
+cudaError_t launch_coarsest_solve_f32(const float* Linv, const float* LinvT, int n, const double* b, double* tmp,
+                                      double* x, const int* guard, cudaStream_t s) {
+  const int blocks = div_up((int64_t)n * 32, 256);
+  tri_matvec_kernel<0, float><<<blocks, 256, 0, s>>>(Linv, n, b, tmp, guard);
+  tri_matvec_kernel<1, float><<<blocks, 256, 0, s>>>(LinvT, n, tmp, x, guard);
   return sf_launched(2);
 }
 

@@ -38,10 +38,14 @@ __device__ __forceinline__ void block_sum(double (&v)[ND], double* sh /*32*ND*/)
   }
 }
 
-// Finalisation by the last block: out[k] = sum of partials in block order.
+// Finalisation by the last block to finish: out[k] = sum of the partials in
+// block order (bitwise reproducible).  The block first stages every partial
+// in shared memory with one parallel round of loads, so the ordered sum runs
+// over shared memory instead of a serial chain of global loads.
 template <int ND>
 __device__ __forceinline__ bool last_block_finalize(const double (&v)[ND], RedWork w, double* out) {
   __shared__ bool is_last;
+  __shared__ double stage[4 * kRedBlocks];
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < ND; ++k) w.partials[k * kRedBlocks + blockIdx.x] = v[k];
@@ -51,11 +55,17 @@ __device__ __forceinline__ bool last_block_finalize(const double (&v)[ND], RedWo
   }
   __syncthreads();
   if (!is_last) return false;
+  __threadfence();
+  const int nb = (int)gridDim.x;
+  for (int e = threadIdx.x; e < ND * nb; e += blockDim.x) {
+    const int k = e / nb, b = e - k * nb;
+    stage[k * kRedBlocks + b] = ((volatile double*)w.partials)[k * kRedBlocks + b];
+  }
+  __syncthreads();
   if (threadIdx.x < ND) {
-    __threadfence();
     const int k = threadIdx.x;
     double s = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) s += ((volatile double*)w.partials)[k * kRedBlocks + b];
+    for (int b = 0; b < nb; ++b) s += stage[k * kRedBlocks + b];
     out[k] = s;
   }
   if (threadIdx.x == 0) *w.ticket = 0u;

@@ -427,13 +427,22 @@ __global__ void restrict_kernel(Grid gf, Grid gc, const double* __restrict__ wx,
   if (n >= gc.nn) return;
   int I, J, K;
   node_ijk(gc, n, I, J, K);
+  // per-axis weights of the three fine nodes 2I - 1 .. 2I + 1 (0 outside the grid)
+  double pw[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int fi = 2 * I + a - 1, fj = 2 * J + a - 1, fk = 2 * K + a - 1;
+    pw[0][a] = (fi < 0 || fi > gf.nx) ? 0.0 : w1(wx, fi, I);
+    pw[1][a] = (fj < 0 || fj > gf.ny) ? 0.0 : w1(wy, fj, J);
+    pw[2][a] = (fk < 0 || fk > gf.nz) ? 0.0 : w1(wz, fk, K);
+  }
   T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
   for (int d = 0; d < 27; ++d) {
-    const int fi = 2 * I + d / 9 - 1, fj = 2 * J + (d / 3) % 3 - 1, fk = 2 * K + d % 3 - 1;
-    if (fi < 0 || fj < 0 || fk < 0 || fi > gf.nx || fj > gf.ny || fk > gf.nz) continue;
-    const T p = (T)(w1(wx, fi, I) * w1(wy, fj, J) * w1(wz, fk, K));
+    const int ax = d / 9, ay = (d / 3) % 3, az = d % 3;
+    const T p = (T)(pw[0][ax] * pw[1][ay] * pw[2][az]);
     if (p == T(0)) continue;
-    const int64_t f = node_id(gf, fi, fj, fk);
+    const int64_t f = node_id(gf, 2 * I + ax - 1, 2 * J + ay - 1, 2 * K + az - 1);
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[c] += p * fine[3 * f + c];
   }
@@ -451,11 +460,20 @@ __global__ void prolong_kernel(Grid gf, Grid gc, const double* __restrict__ wx, 
   int i, j, k;
   node_ijk(gf, f, i, j, k);
   T acc[3] = {T(0), T(0), T(0)};
+  // per-axis weights of the coarse parents floor(i/2) and floor(i/2) + 1 (0 outside)
+  double qw[3][2];
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    const int I = (i >> 1) + b, J = (j >> 1) + b, K = (k >> 1) + b;
+    qw[0][b] = I > gc.nx ? 0.0 : w1(wx, i, I);
+    qw[1][b] = J > gc.ny ? 0.0 : w1(wy, j, J);
+    qw[2][b] = K > gc.nz ? 0.0 : w1(wz, k, K);
+  }
   // coarse parents: floor(i/2) and floor(i/2)+1 (the latter only for odd i)
+#pragma unroll
   for (int a = 0; a < 8; ++a) {
     const int I = (i >> 1) + (a >> 2), J = (j >> 1) + ((a >> 1) & 1), K = (k >> 1) + (a & 1);
-    if (I > gc.nx || J > gc.ny || K > gc.nz) continue;
-    const T p = (T)(w1(wx, i, I) * w1(wy, j, J) * w1(wz, k, K));
+    const T p = (T)(qw[0][a >> 2] * qw[1][(a >> 1) & 1] * qw[2][a & 1]);
     if (p == T(0)) continue;
     const int64_t n = node_id(gc, I, J, K);
 #pragma unroll

@@ -49,7 +49,7 @@ METRIC = "guarded solves/s & s/solve to true resid 1e-6 @512k elems: mixed vs FP
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--steps", type=int, default=48)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--stack", default="plain", choices=["plain", "canonical"])

@@ -2,6 +2,7 @@
 
     python profile_kernels.py smoother-step NX NY NZ [REPS] [--stack plain|canonical] [--precision fp32|fp64]
     python profile_kernels.py dense N [REPS] [--band BW]
+    python profile_kernels.py policy NX NY NZ [--restart R] [--precision mixed|fp64]
 
 smoother-step: builds the 4-level hierarchy on an NX x NY x NZ cantilever
 (random E in [1e-3, 1.001)), then times REPS fused fine smoothing steps with
@@ -10,7 +11,12 @@ pseudo-random vectors) and prints the average launch time and the algorithmic
 bandwidth.  dense: factors and inverts a random SPD N x N matrix (banded with
 lower bandwidth BW when --band is given, as the coarsest level is) with
 simpfem_dense_cholesky_inverse REPS times and prints the best time.
-Both exit 0 on success, so the same command line can run under ncu afterwards.
+policy: one guarded solve of the plain-stack policy on the NX x NY x NZ cantilever
+(seeded void p = 0.35 state, cone filter r = 1.5, SIMP p = 3) after three warm-up
+states, bracketed by cudaProfilerStart/Stop so that `ncu --profile-from-start off`
+sees exactly that solve; --restart bounds the FGMRES basis (device memory) of
+the capture.  All exit 0 on success, so the same command line can run under ncu
+afterwards.
 """
 
 from __future__ import annotations
@@ -94,6 +100,40 @@ def dense(a) -> None:
         print(f"dense n={n} band={a.band}: best {best:.3f} ms over {a.reps}")
 
 
+def policy(a) -> None:
+    import numpy as np
+    import torch
+
+    from gpu_fem.paper4 import PLAIN_JACOBI_STACK
+    from gpu_fem.policy import GuardedFloorPolicy
+    from gpu_fem.presets import cantilever_spec
+    from gpu_fem.pub_simp_solver import _build_density_filter
+
+    nx, ny, nz = a.nx, a.ny, a.nz
+    H = _build_density_filter(nx, ny, 1.5, nz)
+    mixed = a.precision == "mixed"
+    stack = dict(PLAIN_JACOBI_STACK, fine_smoother="fp32" if mixed else "fp64")
+    pol = GuardedFloorPolicy(cantilever_spec(nx, ny, nz), penal=3.0, tol=1e-6, restart=a.restart,
+                             maxiter=a.restart, probe_iters=100, probe_r50=50, raised_rho_mins=(1e-3, 1e-2),
+                             stack=stack, cycle_precision="fp32" if mixed else "fp64")
+
+    def state(seed):
+        solid = (np.random.default_rng(seed).random(nx * ny * nz) >= 0.35).astype(np.float64)
+        return torch.as_tensor(np.asarray(H @ solid), device="cuda")
+
+    for seed in range(3):
+        pol.run(state(seed))
+    d = state(3)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    r = pol.run(d)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(f"policy {a.precision} {nx}x{ny}x{nz}: {r['total_iters']} iterations, floor {r['recommended_rho_min']:.0e}, "
+          f"setup {r['probe_setup_time_s'] * 1e3:.2f} ms, solve {r['probe_solve_time_s'] * 1e3:.2f} ms, "
+          f"guarded {r['solve_converged']}")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -108,8 +148,14 @@ def main() -> None:
     d.add_argument("n", type=int)
     d.add_argument("reps", type=int, nargs="?", default=5)
     d.add_argument("--band", type=int, default=None)
+    q = sub.add_parser("policy")
+    q.add_argument("nx", type=int)
+    q.add_argument("ny", type=int)
+    q.add_argument("nz", type=int)
+    q.add_argument("--restart", type=int, default=300)
+    q.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     a = ap.parse_args()
-    smoother_step(a) if a.cmd == "smoother-step" else dense(a)
+    {"smoother-step": smoother_step, "dense": dense, "policy": policy}[a.cmd](a)
 
 
 if __name__ == "__main__":

@@ -10,12 +10,16 @@ radius 1.5, E = 1e-12 + (1 - 1e-12) rho_f^3, unit tip load, x = 0 face clamped.
 The hierarchy is the damped-Jacobi V-cycle (4 levels, FGMRES restart 300,
 tol 1e-6); ``--stack canonical`` selects the reference drivers' default stack.
 
-The mixed arm (``value``, ``e2e``) is the mixed-precision, batched form:
-``--width`` states in flight per GPU (gpu_fem.policy.BatchedFloorPolicy, one
-hierarchy and CUDA stream per worker).  The ``fp64`` object is the plain FP64
-form from scratch, one state at a time, on the same states.
+The mixed arm (``value``, ``e2e``) is the mixed-precision, batched and learned
+form: ``--width`` states in flight per GPU (gpu_fem.policy.BatchedFloorPolicy,
+one hierarchy and CUDA stream per worker), each worker a LearnedFloorPolicy
+with the committed floor proposer (``--policy plain`` for the probe-and-ladder
+alone); ``learned_stops_at_r50`` counts the states whose probe the proposal or
+the r50 rule ended early.  The ``fp64`` object is the plain FP64 form from
+scratch, one state at a time, on the same states.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--width B] [--impl native|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--width B] [--policy learned|plain]
+                    [--impl native|reference]
 
 N > 1 (torchrun): ranks solve disjoint states, no collective on the data path;
 the reported value is all states / max-over-ranks time.
@@ -54,6 +58,8 @@ def _args():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--stack", default="plain", choices=["plain", "canonical"])
     ap.add_argument("--width", type=int, default=4, help="states in flight per GPU in the mixed arm")
+    ap.add_argument("--policy", default="learned", choices=["learned", "plain"],
+                    help="mixed arm: learned floor proposal (decides at r50) or the plain probe-and-ladder")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -190,7 +196,7 @@ def run_native(args):
     H = _filter()
     spec = cantilever_spec(NX, NY, NZ)
     K, W, B = args.steps, args.warmup, max(1, args.width)
-    WB = max(W, B)  # warm-up states for the batched arm: every worker sees at least one
+    WB = max(W, 2 * B)  # warm-up states for the batched arm: every worker sees at least two
     seeds = [1000 * rank + i for i in range(WB + 2 * K)]
     states = {s: make_state(H, s) for s in seeds}
 
@@ -262,7 +268,12 @@ def run_native(args):
         return ms, rows, launches
 
     # mixed precision, B states in flight (one hierarchy and stream per worker)
-    mixed = BatchedFloorPolicy(B, spec, **policy_kwargs("mixed"))
+    learned = None
+    if args.policy == "learned":
+        from gpu_fem.floor_proposer import DEFAULT_WEIGHTS
+
+        learned = DEFAULT_WEIGHTS
+    mixed = BatchedFloorPolicy(B, spec, learned=learned, **policy_kwargs("mixed"))
     mixed.run_many([torch.as_tensor(states[s], device="cuda") for s in seeds[:WB]])
     timed_seeds = seeds[WB:WB + K]
     with ClockSampler(local) as clk:
@@ -329,6 +340,8 @@ def run_native(args):
             for s, r, f in zip(timed_seeds, rows_mixed, rows_fp64)
         ],
         "all_guarded": all(r["solve_converged"] for r in rows_mixed + rows_e2e + rows_fp64),
+        "policy": args.policy,
+        "learned_stops_at_r50": sum(1 for r in rows_mixed + rows_e2e if r.get("stopped_at_r50")),
         "e2e": {
             "value": round(e2e_value, 4),
             "unit": "guarded solves/s",

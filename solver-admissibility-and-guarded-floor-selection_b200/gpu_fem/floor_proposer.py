@@ -193,9 +193,11 @@ class LearnedFloorPolicy(GuardedFloorPolicy):
     raised rungs above it, the raised rungs below it, and -- when the stop was the
     proposer's and not the high-residual rule's -- the baseline floor last."""
 
-    def __init__(self, preset, *, proposer: FloorProposerNet, dims: Sequence[int], min_confidence: float = 0.5,
-                 **kwargs):
+    def __init__(self, preset, *, proposer: FloorProposerNet, dims: Optional[Sequence[int]] = None,
+                 min_confidence: float = 0.5, **kwargs):
         super().__init__(preset, **kwargs)
+        if dims is None:
+            dims = (self.spec.nelx, self.spec.nely, self.spec.nelz)
         rungs = [self.baseline_rho_min] + list(self.raised_rho_mins)
         if tuple(rungs) != RUNGS:
             raise ValueError("the proposer is trained on the rungs 1e-12 | 1e-3, 1e-2")
@@ -261,8 +263,16 @@ class LearnedFloorPolicy(GuardedFloorPolicy):
                 break
         if sel is probe:
             self.last_x = probe_x
+        failed = [a for a in attempts if a is not sel]
         return {
             "probe_r50": r50, "probe_r100": r100, "probe_iters": probe.iters, "probe_history": probe_history,
+            "probe_setup_time_s": probe.setup_time_s, "probe_solve_time_s": probe.solve_time_s,
+            "selected_reused_probe": int(sel is probe),
+            "selected_setup_time_s": sel.setup_time_s if sel else float("nan"),
+            "selected_solve_time_s": sel.solve_time_s if sel else float("nan"),
+            "failed_ladder_setup_time_s": sum(a.setup_time_s for a in failed),
+            "failed_ladder_solve_time_s": sum(a.solve_time_s for a in failed),
+            "solver_reported_converged": int(bool(sel and sel.solver_reported_converged)),
             "trigger": trigger, "predicted_raise_floor": int(raise_floor), "stopped_at_r50": dec["stop"] or "",
             "proposal": -1 if dec["proposed"] is None else dec["proposed"],
             "proposal_prob": [] if dec["prob"] is None else dec["prob"].tolist(),
@@ -276,4 +286,7 @@ class LearnedFloorPolicy(GuardedFloorPolicy):
             "total_iters": probe.iters + sum(a.iters for a in attempts if a is not probe),
             "policy_time_s": pool_time + probe.setup_time_s + probe.solve_time_s
             + sum(a.setup_time_s + a.solve_time_s for a in attempts if a is not probe),
+            "recorded_policy_time_s": probe.setup_time_s + probe.solve_time_s
+            + sum(a.setup_time_s + a.solve_time_s for a in attempts if a is not probe),
+            "attempts": attempts,
         }

@@ -217,9 +217,13 @@ class BatchedFloorPolicy:
     to worker k mod width and each worker takes its states in order, so results
     are deterministic; every worker carries its own lambda-cache history, as one
     driver hierarchy does.  Every accepted answer still passes the FP64 guard.
+
+    ``learned``: path of floor-proposer weights (gpu_fem.floor_proposer); the
+    workers are then LearnedFloorPolicy instances, each with its own network
+    handle (a handle's workspaces serve one stream at a time).
     """
 
-    def __init__(self, width: int = 3, *args, **kwargs):
+    def __init__(self, width: int = 3, *args, learned: Optional[str] = None, **kwargs):
         torch = _lib.require_cuda()
         if int(width) < 1:
             raise ValueError("width must be >= 1")
@@ -228,7 +232,13 @@ class BatchedFloorPolicy:
         for i in range(self.width):
             # private mesh handles: scratch and reduction workspaces are per handle
             with mesh_namespace(("batched", id(self), i)):
-                self.workers.append(GuardedFloorPolicy(*args, **kwargs))
+                if learned is None:
+                    self.workers.append(GuardedFloorPolicy(*args, **kwargs))
+                else:
+                    from .floor_proposer import FloorProposerNet, LearnedFloorPolicy
+
+                    net = FloorProposerNet.load(learned, max_batch=1)
+                    self.workers.append(LearnedFloorPolicy(*args, proposer=net, **kwargs))
         self.streams = [torch.cuda.Stream() for _ in range(self.width)]
         # pick the sweep shapes now, on an idle device; every worker's mesh (same
         # grid) then reuses them

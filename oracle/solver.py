@@ -361,3 +361,29 @@ def fixed_pcg(K, b, d_inv, n_iters):
         p = z + (rzn / (rz + 1e-300)) * p
         rz = rzn
     return x
+
+
+def _bf16_round(x: np.ndarray) -> np.ndarray:
+    """float32 -> bfloat16 (round to nearest, ties to even) -> float32."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32).view(np.float32)
+
+
+def fused_matvec_full(nx: int, ny: int, nz: int, u_full: np.ndarray, E: np.ndarray, ke: np.ndarray,
+                      dtype: str = "fp32") -> np.ndarray:
+    """The reference's FusedMatvec arithmetic (gpu_fem/cuda_fused_matvec.py:41-88
+    FP32, :112-246 BF16 WMMA, :343-416 wrapper): per element f_e = KE u_e with u and
+    KE cast to float32 (and, for "bf16", rounded to bfloat16), times E_e (float32),
+    scatter-added into every DOF of the full vector.  Evaluated in float64 here;
+    the kernels accumulate in float32."""
+    edof = edof_table(nx, ny, nz)
+    u32 = np.asarray(u_full, dtype=np.float32)
+    k32 = np.asarray(ke, dtype=np.float32)
+    if dtype == "bf16":
+        u32, k32 = _bf16_round(u32), _bf16_round(k32)
+    elif dtype != "fp32":
+        raise ValueError(dtype)
+    U = u32.astype(np.float64)[edof]
+    F = U @ k32.astype(np.float64).T
+    F *= np.asarray(E, dtype=np.float32).astype(np.float64)[:, None]
+    return np.bincount(edof.ravel(), weights=F.ravel(), minlength=u32.size)

@@ -135,3 +135,21 @@ def test_restart_rule_and_pcg(ref):
     hist = []
     S.pcg(lambda v: op.matvec(v, E), F, g.apply, tol=1e-6, maxiter=200, history=hist)
     np.testing.assert_allclose(hist[:10], ref[f"{name}/pcg_plain_hist"][:10], rtol=1e-9)
+
+
+def test_fused_matvec_restatement_matches_operator():
+    """The oracle's FusedMatvec arithmetic (float32 casts of u, KE, E) equals the
+    FP64 operator on an all-free mesh to float32 rounding, and its BF16 variant
+    only by bfloat16 rounding."""
+    from oracle import solver as s
+
+    dims = (6, 4, 3)
+    nd = 3 * 7 * 5 * 4
+    rng = np.random.default_rng(0)
+    u = rng.standard_normal(nd)
+    E = rng.random(6 * 4 * 3) + 0.1
+    a = s.Operator(*dims, np.arange(nd)).matvec(u, E)
+    b = s.fused_matvec_full(*dims, u, E, s.ke_unit_3d(), "fp32")
+    c = s.fused_matvec_full(*dims, u, E, s.ke_unit_3d(), "bf16")
+    assert np.abs(a - b).max() <= 1e-6 * np.abs(a).max()
+    assert 1e-5 < np.abs(a - c).max() / np.abs(a).max() < 3e-2

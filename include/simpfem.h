@@ -15,6 +15,7 @@
 #ifndef SIMPFEM_H
 #define SIMPFEM_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #if defined(__GNUC__)
@@ -205,6 +206,29 @@ int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, dou
  * *info_host: 0 on success, else the 1-based index of the first non-positive or
  * non-finite pivot, or n + 1 when L^{-1} holds a non-finite entry. */
 int simpfem_dense_cholesky_inverse(int n, double* A, double* Linv, int* info_host, void* stream);
+
+/* ---- SIMP loop around the guarded solve ------------------------------------------
+ * y = H x (transpose 0) or H^T x (transpose 1) for the row-normalised cone density
+ * filter of radius rmin in [1, 3.5] on an nx x ny x nz element grid (weights
+ * rmin - dist within distance < rmin, the element itself rmin; replaces
+ * _build_density_filter's sparse matrix and its SpMVs, pub_simp_solver.py:90-117,
+ * simp_gpu.py:212-294).  x and y are device arrays of nx*ny*nz doubles, x != y. */
+int simpfem_cone_filter(int nx, int ny, int nz, double rmin, int transpose, const double* x, double* y,
+                        void* stream);
+/* Bytes of device workspace simpfem_oc_update needs (the caller allocates it). */
+size_t simpfem_oc_work_bytes(void);
+/* The optimality-criteria update of _oc_step_cupy (simp_gpu.py:212-294) without a
+ * Heaviside projection: bisection on the multiplier over [0, 1e9] (at most 100
+ * steps, until the bracket is below 1e-9) of
+ * rn = clip(clip(rho sqrt(-min(dc,-1e-12) / (lm max(dv,1e-12))), rho -+ move), 1e-3, 1)
+ * against sum(H rn) = volfrac n, evaluated as sum_j dv_j rn_j with dv = H^T 1.
+ * rho, dc, dv, rho_new: device arrays of n doubles; work: device workspace of at
+ * least simpfem_oc_work_bytes() bytes.  *change_host = max |rho_new - rho|,
+ * *lambda_host the final multiplier, *steps_host the bisection steps (each may be
+ * NULL).  Synchronises the stream once per bisection step. */
+int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const double* dv, double volfrac,
+                      double move, double* rho_new, double* work, size_t work_bytes, double* change_host,
+                      double* lambda_host, int* steps_host, void* stream);
 
 /* ---- learned floor proposer (no counterpart in the reference) ------------------
  * A small 3D CNN over the density pooled to 16^3 plus two probe features, with a

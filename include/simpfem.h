@@ -182,16 +182,22 @@ int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, 
                    double tol, int maxiter, int restart, double* history_host, int history_cap,
                    int* history_len, int* iters, int* converged, void* stream);
 /* simpfem_fgmres with a host check, no counterpart in the reference (the learned
- * floor policy decides at the probe's r50 point with it): once the solve has
- * completed check_iter iterations and is still running, check_fn(check_ctx,
- * check_iter, history, history_len) is called on the calling thread with the
- * relative-residual history so far; a nonzero return ends the solve there, with
+ * floor policy decides at the probe's r50 point with it, and the checkpointed
+ * guard -- the reference README's proposed extension -- reads the true residual
+ * there): once the solve has completed check_iter iterations and is still
+ * running, check_fn(check_ctx, check_iter, history, history_len, true_rel) is
+ * called on the calling thread with the relative-residual history so far and,
+ * when check_true_residual is nonzero, the FP64 true relative residual
+ * ||b - A x|| / ||b|| of the iterate formed at that point (NaN otherwise; the
+ * solve itself is not changed).  A nonzero return ends the solve there, with
  * x_free the iterate after check_iter iterations, *converged 0 and *stopped 1.
  * check_iter < 1 or check_fn NULL is simpfem_fgmres.  stopped may be NULL. */
 int simpfem_fgmres_checked(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
                            double tol, int maxiter, int restart, double* history_host, int history_cap,
                            int* history_len, int* iters, int* converged, int check_iter,
-                           int (*check_fn)(void* ctx, int iters, const double* history, int history_len),
+                           int check_true_residual,
+                           int (*check_fn)(void* ctx, int iters, const double* history, int history_len,
+                                           double true_rel_residual),
                            void* check_ctx, int* stopped, void* stream);
 /* PCG with the hierarchy as preconditioner (_cupy_pcg, gpu_fem/solver_v2.py:551-623). */
 int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,

@@ -375,7 +375,9 @@ int simpfem_gmg_fine_E(simpfem_gmg* g, const double** E_out) {
 int simpfem_fgmres_checked(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
                            double tol, int maxiter, int restart, double* history_host, int history_cap,
                            int* history_len, int* iters, int* converged, int check_iter,
-                           int (*check_fn)(void* ctx, int iters, const double* history, int history_len),
+                           int check_true_residual,
+                           int (*check_fn)(void* ctx, int iters, const double* history, int history_len,
+                                           double true_rel_residual),
                            void* check_ctx, int* stopped, void* stream) {
   SF_API_BEGIN
   if (!g || !b_free || !x_free) throw InvalidArg{"simpfem_fgmres: null argument"};
@@ -395,6 +397,7 @@ int simpfem_fgmres_checked(simpfem_gmg* g, const double* b_free, const double* x
   PrecFn M = [&G](const double* in, double* out, const int* guard) { apply_full(G, in, out, guard); };
   CheckHook hook;
   hook.iter = check_iter;
+  hook.true_residual = check_true_residual ? 1 : 0;
   hook.fn = check_iter >= 1 ? check_fn : nullptr;
   hook.ctx = check_ctx;
   run_outer_fgmres(G, g->bfull.as<double>(), g->xfull.as<double>(), x0_free == nullptr, tol, maxiter, restart, M,
@@ -419,7 +422,7 @@ int simpfem_fgmres(simpfem_gmg* g, const double* b_free, const double* x0_free, 
                    int maxiter, int restart, double* history_host, int history_cap, int* history_len, int* iters,
                    int* converged, void* stream) {
   return simpfem_fgmres_checked(g, b_free, x0_free, x_free, tol, maxiter, restart, history_host, history_cap,
-                                history_len, iters, converged, -1, nullptr, nullptr, nullptr, stream);
+                                history_len, iters, converged, -1, 0, nullptr, nullptr, nullptr, stream);
 }
 
 int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free, double tol,

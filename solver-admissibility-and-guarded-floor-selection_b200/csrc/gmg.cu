@@ -832,11 +832,32 @@ static void fgmres(Gmg& G, KrylovWs& K, const double* b, double* x, bool x0_zero
         // it sees the residual history so far and may end the solve here; the
         // iterate after these columns is then formed as at the end of a cycle
         if (check && check->fn && K.hflags()[F_TOTAL] == check->iter && hist_dev) {
+          double true_rel = NAN;
+          if (check->true_residual) {
+            // the iterate after these columns, formed in the free restart-residual
+            // vector (the back-solve writes only y), and its FP64 true residual in w
+            SF_CUDA(launch_backsolve(kd, G.st));
+            SF_CUDA(launch_copy(F64, n, x, K.r.p, nullptr, G.st));
+            SF_CUDA(launch_update_x(n, K.r.as<double>(), (double* const*)K.Zptr.p, kd.y, kd.flags, G.st));
+            EpiArgs ea;
+            ea.y = K.w.p;
+            ea.b = b;
+            fine_apply(m, F64, EPI_RESID, G.E64.p, K.r.p, ea, G.st);
+            DotSet ds;
+            ds.a[0] = K.w.p;
+            ds.b[0] = K.w.p;
+            ds.nd = 1;
+            dots(G, F64, n, ds, kd.sc + 8, nullptr);
+            double sc[9];
+            SF_CUDA(cudaMemcpyAsync(sc, kd.sc, sizeof(sc), cudaMemcpyDeviceToHost, G.st));
+            SF_CUDA(cudaStreamSynchronize(G.st));
+            true_rel = sc[SC_BNORM] > 0.0 ? sqrt(sc[8]) / sc[SC_BNORM] : 0.0;
+          }
           const int hn = std::min(K.hflags()[F_HISTN], hist_cap);
           check->buf.resize(hn);
           SF_CUDA(cudaMemcpyAsync(check->buf.data(), hist_dev, sizeof(double) * hn, cudaMemcpyDeviceToHost, G.st));
           SF_CUDA(cudaStreamSynchronize(G.st));
-          if (check->fn(check->ctx, check->iter, check->buf.data(), hn)) {
+          if (check->fn(check->ctx, check->iter, check->buf.data(), hn, true_rel)) {
             stopped = true;
             check->stopped = true;
             break;

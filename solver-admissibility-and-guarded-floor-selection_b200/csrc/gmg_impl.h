@@ -217,11 +217,14 @@ Gmg* gmg_create(Mesh* m, const simpfem_gmg_opts& o);
 void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free);
 void apply_full(Gmg& G, const double* rhs, double* out, const int* guard);
 // A host check called once, when the outer FGMRES has completed ``iter``
-// iterations and is still running: fn(ctx, iter, history, history_len) sees the
-// relative-residual history so far and returns nonzero to end the solve there.
+// iterations and is still running: fn(ctx, iter, history, history_len,
+// true_rel) sees the relative-residual history so far (and, with
+// true_residual set, ||b - A x_iter|| / ||b|| of the iterate formed at that
+// point, else NaN) and returns nonzero to end the solve there.
 struct CheckHook {
   int iter = -1;
-  int (*fn)(void* ctx, int iters, const double* history, int history_len) = nullptr;
+  int true_residual = 0;
+  int (*fn)(void* ctx, int iters, const double* history, int history_len, double true_rel) = nullptr;
   void* ctx = nullptr;
   mutable std::vector<double> buf;
   mutable bool stopped = false;

@@ -111,7 +111,7 @@ _SIGS = {
     "simpfem_gmg_reset_lambda_cache": (_I, [_P]),
     "simpfem_gmg_fine_E": (_I, [_P, _P]),
     "simpfem_fgmres": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _P]),
-    "simpfem_fgmres_checked": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _I, _P, _P, _P, _P]),
+    "simpfem_fgmres_checked": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
     "simpfem_pcg": (_I, [_P, _P, _P, _P, _D, _I, _P, _I, _P, _P, _P, _P]),
     "simpfem_dense_cholesky_inverse": (_I, [_I, _P, _P, _P, _P]),
     "simpfem_cone_filter": (_I, [_I, _I, _I, _D, _I, _P, _P, _P]),

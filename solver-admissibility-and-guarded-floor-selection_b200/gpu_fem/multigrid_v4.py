@@ -29,9 +29,9 @@ from ._native import to_numpy
 from .solver_v2 import MatrixFreeKff, _native_gmg
 
 _PREC = {"fp64": _lib.F64, "fp32": _lib.F32, "bf16": _lib.BF16}
-# int check(void* ctx, int iters, const double* history, int history_len)
+# int check(void* ctx, int iters, const double* history, int history_len, double true_rel_residual)
 _CHECK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
-                             ctypes.c_int)
+                             ctypes.c_int, ctypes.c_double)
 _PREC_NAME = {v: k for k, v in _PREC.items()}
 _ENRICH = {"none": 0, "weighted_residual_second": 1, "weighted_gap_second": 2, "void_residual_second": 3,
            "void_gap_second": 4}
@@ -403,9 +403,12 @@ class GalerkinMatFreeGMG:
 
     # ------------------------------------------------------------ native Krylov
     def _native_fgmres(self, b, x0, tol, maxiter, restart, history, check=None):
-        """``check``: optional (iteration, fn); fn(history_so_far) runs once when the
-        solve has completed that many iterations and is still running, and a true
-        return ends the solve there (the result then reports not converged)."""
+        """``check``: optional (iteration, fn) or (iteration, fn, True); fn runs once
+        when the solve has completed that many iterations and is still running --
+        fn(history_so_far), or with the third element fn(history_so_far,
+        true_rel_residual) where true_rel_residual is the FP64 true relative
+        residual of the iterate at that point -- and a true return ends the solve
+        there (the result then reports not converged)."""
         torch = _lib.require_cuda()
         bb = _lib.as_cuda(b, torch.float64)
         x = torch.empty_like(bb)
@@ -419,12 +422,14 @@ class GalerkinMatFreeGMG:
                       _lib.ptr(x), float(tol), int(maxiter), int(restart), hist.ctypes.data_as(ctypes.c_void_p), cap,
                       ctypes.byref(hlen), ctypes.byref(it), ctypes.byref(conv), _lib.stream_ptr())
         else:
-            check_iter, fn = check
+            check_iter, fn = check[0], check[1]
+            want_true = len(check) > 2 and bool(check[2])
             errors = []
 
-            def trampoline(_ctx, _iters, hptr, hn):
+            def trampoline(_ctx, _iters, hptr, hn, true_rel):
                 try:
-                    return 1 if fn([float(hptr[k]) for k in range(hn)]) else 0
+                    hist_now = [float(hptr[k]) for k in range(hn)]
+                    return 1 if (fn(hist_now, float(true_rel)) if want_true else fn(hist_now)) else 0
                 except BaseException as e:  # raised again once the call returns
                     errors.append(e)
                     return 0
@@ -433,7 +438,7 @@ class GalerkinMatFreeGMG:
             stopped = ctypes.c_int()
             _lib.call("simpfem_fgmres_checked", self._h, _lib.ptr(bb), _lib.ptr(x0t) if x0t is not None else None,
                       _lib.ptr(x), float(tol), int(maxiter), int(restart), hist.ctypes.data_as(ctypes.c_void_p), cap,
-                      ctypes.byref(hlen), ctypes.byref(it), ctypes.byref(conv), int(check_iter),
+                      ctypes.byref(hlen), ctypes.byref(it), ctypes.byref(conv), int(check_iter), int(want_true),
                       ctypes.cast(cb, ctypes.c_void_p), None, ctypes.byref(stopped), _lib.stream_ptr())
             if errors:
                 raise errors[0]

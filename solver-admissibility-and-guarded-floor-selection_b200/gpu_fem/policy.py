@@ -60,7 +60,7 @@ class GuardedFloorPolicy:
                  high_residual_threshold: float = 1e-2, plateau_residual_threshold: float = 1e-4,
                  plateau_ratio_threshold: float = 0.6, severity_jump_r50_threshold: float = 0.0,
                  severity_jump_rho_min: float = 1e-2, stack: Optional[dict] = None, n_levels: int = 4,
-                 cycle_precision: str = "fp64", reuse_probe: bool = True):
+                 cycle_precision: str = "fp64", reuse_probe: bool = True, checkpoint_guard: bool = False):
         flags = dict(CANONICAL_STACK if stack is None else stack)
         (self.spec, self.bc, self.free, self.free_gpu, self.edof_gpu, self.F_free_gpu, self.mf_op,
          self.gmg) = _build_components(preset, n_levels=n_levels, cycle_precision=cycle_precision, **flags)
@@ -80,6 +80,10 @@ class GuardedFloorPolicy:
         self.severity_jump_rho_min = float(severity_jump_rho_min)
         self.b_norm = float(torch.linalg.norm(self.F_free_gpu))
         self.reuse_probe = bool(reuse_probe)
+        # checkpointed guard (the reference README's proposed extension): the probe
+        # recomputes the FP64 true residual of its iterate at r50, and the rule reads
+        # true residuals at r50 and at the probe's end instead of FGMRES's estimates
+        self.checkpoint_guard = bool(checkpoint_guard)
         self.last_x = None
 
     # ---------------------------------------------------------------- moduli
@@ -130,11 +134,26 @@ class GuardedFloorPolicy:
     # ---------------------------------------------------------------- policy
     def run(self, density, *, binary: bool = False) -> dict:
         probe_history: list = []
+        chk: dict = {}
+        check = None
+        if self.checkpoint_guard:
+            def at_r50(_history, true_rel):
+                chk["r50"] = true_rel
+                return False  # observe only
+
+            check = (self.probe_r50, at_r50, True)
         probe = self.solve_at_floor(density, self.baseline_rho_min, maxiter=self.probe_iters,
-                                    history=probe_history, binary=binary)
+                                    history=probe_history, binary=binary, check=check)
         r50 = probe_history[min(self.probe_r50, len(probe_history) - 1)]
         r100 = probe_history[min(self.probe_iters, len(probe_history) - 1)]
-        raise_floor, trigger = _classify(r50, r100, **self.thresholds)
+        true_r50 = true_r100 = float("nan")
+        if self.checkpoint_guard:
+            # a probe that stopped before r50 has one true residual, at its end
+            true_r50 = float(chk.get("r50", probe.final_rel_residual))
+            true_r100 = float(probe.final_rel_residual)
+            raise_floor, trigger = _classify(true_r50, true_r100, **self.thresholds)
+        else:
+            raise_floor, trigger = _classify(r50, r100, **self.thresholds)
         severity = raise_floor and self.severity_jump_r50_threshold > 0.0 and r50 >= self.severity_jump_r50_threshold
         if raise_floor and severity:
             ladder = [v for v in self.raised_rho_mins if v >= self.severity_jump_rho_min] or [self.severity_jump_rho_min]
@@ -177,6 +196,9 @@ class GuardedFloorPolicy:
             "probe_r50": r50,
             "probe_r100": r100,
             "probe_r100_over_r50": r100 / max(r50, 1e-300),
+            "checkpoint_guard": int(self.checkpoint_guard),
+            "probe_true_r50": true_r50,
+            "probe_true_r100": true_r100,
             "probe_setup_time_s": probe.setup_time_s,
             "probe_solve_time_s": probe.solve_time_s,
             "probe_iters": probe.iters,

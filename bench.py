@@ -64,6 +64,28 @@ def _args():
     return ap.parse_args()
 
 
+def rank_seeds(rank: int, n: int) -> list:
+    """State seeds of one rank: disjoint across ranks (replicas shard the states)."""
+    return [1000 * rank + i for i in range(n)]
+
+
+def job_states(per_rank: int, world: int) -> int:
+    """States the whole job solves in the timed region (weak scaling)."""
+    return per_rank * world
+
+
+def max_over_ranks(ms: float, world: int, device: str) -> float:
+    """The job's time: the slowest rank's device time (one all-reduce MAX)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _filter():
     from gpu_fem.pub_simp_solver import _build_density_filter
 
@@ -197,7 +219,7 @@ def run_native(args):
     spec = cantilever_spec(NX, NY, NZ)
     K, W, B = args.steps, args.warmup, max(1, args.width)
     WB = max(W, 2 * B)  # warm-up states for the batched arm: every worker sees at least two
-    seeds = [1000 * rank + i for i in range(WB + 2 * K)]
+    seeds = rank_seeds(rank, WB + 2 * K)
     states = {s: make_state(H, s) for s in seeds}
 
     def policy_kwargs(precision):
@@ -232,10 +254,7 @@ def run_native(args):
         barrier()
         ms = e0.elapsed_time(e1)
         launches = _lib.lib().simpfem_launch_count() - l0
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, world, "cuda")
         return ms, rows, launches
 
     def timed_batch(bp, seq, host_io: bool):
@@ -261,10 +280,7 @@ def run_native(args):
         barrier()
         ms = e0.elapsed_time(e1)
         launches = _lib.lib().simpfem_launch_count() - l0
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, world, "cuda")
         return ms, rows, launches
 
     # mixed precision, B states in flight (one hierarchy and stream per worker)
@@ -285,7 +301,7 @@ def run_native(args):
         fp64.run(torch.as_tensor(states[s], device="cuda"))
     ms_fp64, rows_fp64, _ = timed(fp64, timed_seeds, host_io=False)
 
-    n_states = K * world
+    n_states = job_states(K, world)
     value = n_states / (ms_mixed / 1e3)
     e2e_value = n_states / (ms_e2e / 1e3)
     n_free = int(mixed.workers[0].F_free_gpu.numel())

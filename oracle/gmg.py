@@ -218,21 +218,31 @@ class GMG:
     # ------------------------------------------------------------ corrections (:867-1055)
     def correction(self, lv, x, res, c):
         """Returns (x, corrected residual)."""
+        return self.correction_decision(lv, x, res, c)[:2]
+
+    def correction_decision(self, lv, x, res, c):
+        """(x, corrected residual, raw scale, applied scale, note) of the coarse
+        correction (multigrid_v4.py:867-931); raw scale None is kept as None."""
         if self.cc == "none":
-            return x + c, res - self.Alv(lv, c)
+            return x + c, res - self.Alv(lv, c), 1.0, 1.0, ""
         cn, rn = float(np.linalg.norm(c)), float(np.linalg.norm(res))
         if cn <= 1e-300 or rn <= 1e-300:
-            return x, res
+            return x, res, 0.0, 0.0, "degenerate_correction"
         Ac = self.Alv(lv, c)
         den = float(np.dot(Ac, Ac))
         if den <= 1e-300:
-            return x, res
+            return x, res, 0.0, 0.0, "degenerate_correction"
         raw = float(np.dot(res, Ac) / den)
         s = min(self.cc_max, max(0.0, raw))
         trial = res - s * Ac
         if float(np.linalg.norm(trial)) > self.cc_ratio * rn:
-            return x, res
-        return x + s * c, trial
+            return x, res, raw, 0.0, "rejected_correction"
+        note = ""
+        if s <= 1e-12 and raw <= 0.0:
+            note = "nonpositive_correction_scale"
+        elif abs(s - raw) > 1e-12:
+            note = "clipped_correction_scale"
+        return x + s * c, trial, raw, s, note
 
     def enrichment_rhs(self, residual):
         w = self.wenrich
@@ -247,29 +257,37 @@ class GMG:
         return R0 @ (vw * (residual - P0 @ (R0 @ residual)))
 
     def root_local(self, x, residual):
+        return self.root_local_decision(x, residual)[0]
+
+    def root_local_decision(self, x, residual):
+        """(x, residual, raw scale, applied scale, note) of the root-local
+        correction (multigrid_v4.py:964-1055)."""
+        if self.rl == "none":
+            return x, residual, None, 0.0, ""
         if self.rl == "node_block_inner_fgmres":
             corr, _, _ = fgmres(self.A0, residual, self.nbj.apply, tol=0.0, maxiter=self.rl_steps,
                                 restart=self.rl_restart)
             cn, rn = float(np.linalg.norm(corr)), float(np.linalg.norm(residual))
             if cn <= 1e-300 or rn <= 1e-300:
-                return x
+                return x, residual, 0.0, 0.0, "degenerate_root_local_correction"
             trial = residual - self.A0(corr)
             if float(np.linalg.norm(trial)) > rn:
-                return x
-            return x + corr
+                return x, residual, None, 0.0, "rejected_root_local_inner_fgmres"
+            return x + corr, trial, None, 1.0, "root_local_inner_fgmres"
         corr = self.nbj.apply(residual)
         cn, rn = float(np.linalg.norm(corr)), float(np.linalg.norm(residual))
         if cn <= 1e-300 or rn <= 1e-300:
-            return x
+            return x, residual, 0.0, 0.0, "degenerate_root_local_correction"
         Ac = self.A0(corr)
         den = float(np.dot(Ac, Ac))
         if den <= 1e-300:
-            return x
+            return x, residual, 0.0, 0.0, "degenerate_root_local_correction"
         raw = float(np.dot(residual, Ac) / den)
         s = min(self.rl_max, max(0.0, raw))
         if s <= 1e-12:
-            return x
-        return x + s * corr
+            return x, residual, raw, 0.0, "nonpositive_root_local_scale"
+        note = "clipped_root_local_scale" if abs(s - raw) > 1e-12 else ""
+        return x + s * corr, residual - s * Ac, raw, s, note
 
     # ------------------------------------------------------------ cycles (:1929-2024)
     def vcycle(self, lv, rhs):
@@ -321,6 +339,156 @@ class GMG:
         if self.rl != "none":
             x = self.root_local(x, rhs - self.A0(x))
         return x
+
+    # ------------------------------------------------------------ cycle trace (:1362-1728)
+    def cycle_trace(self, rhs, cycle_type=None) -> dict:
+        """One traced base cycle, then the root-local correction: the dictionary
+        of MultigridCycleTrace.to_dict() (multigrid_v4.py:81-113, :1362-1438),
+        visits in pre-order (visit_id).  The inner Krylov wrapper is not traced."""
+        if not self.is_setup:
+            raise RuntimeError("GalerkinMatFreeGMG.setup() must be called before cycle_trace().")
+        cyc = self.cycle if cycle_type is None else cycle_type
+        if cyc not in ("v", "w"):
+            raise ValueError(f"cycle_type must be 'v' or 'w'; got {cyc!r}")
+        rhs = np.asarray(rhs, dtype=np.float64)
+        visits = []
+        out = self._trace_level(0, rhs, visits, [0], cyc)
+        pre = rhs - self.A0(out)
+        out, res, lraw, lapp, lnote = self.root_local_decision(out, pre)
+        visits.sort(key=lambda v: v["visit_id"])
+        if lnote:
+            root = next((v for v in visits if v["level"] == 0 and not v["is_coarsest"]), None)
+            if root is not None:
+                root["notes"] = _merge_notes(root["notes"], lnote)
+        nrm = lambda v: float(np.linalg.norm(v))  # noqa: E731
+        rn, jn, on, resn = nrm(rhs), nrm(self.dinv[0] * rhs), nrm(out), nrm(res)
+        rz = float(np.dot(rhs, out))
+        return {
+            "cycle_type": cyc, "rhs_norm": rn, "jacobi_action_norm": jn, "output_norm": on,
+            "z_over_jacobi": _safe_ratio(on, jn), "rz": rz, "pd": bool(rz > 0.0),
+            "output_residual_norm": resn, "output_residual_ratio": _safe_ratio(resn, rn),
+            "contrast_ratio": self.contrast, "is_high_contrast": self.high,
+            "fine_degree_adapt": self.deg_adapt, "coarse_iters_adapt": self.c_adapt,
+            "coarse_correction_policy": self.cc, "coarse_correction_acceptance_ratio": self.cc_ratio,
+            "coarse_correction_max_scale": self.cc_max, "root_enrichment_mode": self.enrich,
+            "root_enrichment_weight_floor": self.w_floor, "root_enrichment_weight_power": self.w_pow,
+            "root_local_correction_mode": self.rl, "root_local_correction_inner_steps": self.rl_steps,
+            "root_local_correction_inner_restart": self.rl_restart,
+            "root_local_correction_raw_scale": lraw, "root_local_correction_applied_scale": lapp,
+            "root_local_correction_residual_ratio": _safe_ratio(resn, nrm(pre)),
+            "inner_krylov_steps": self.ik, "inner_krylov_restart": self.ik_restart,
+            "visits": visits,
+        }
+
+    def _trace_level(self, lv, rhs, visits, counter, cyc):
+        nrm = lambda v: float(np.linalg.norm(v))  # noqa: E731
+        vid = counter[0]
+        counter[0] += 1
+        rn, jn = nrm(rhs), nrm(self.dinv[lv] * rhs)
+        visit = {"visit_id": vid, "level": lv, "cycle_type": cyc, "rhs_norm": rn, "jacobi_action_norm": jn}
+        if lv == self.L - 1:
+            x = self.solve_coarsest(rhs)
+            resn = nrm(rhs - self.Alv(lv, x))
+            xn = nrm(x)
+            visit.update(is_coarsest=True, n_coarse_corrections=0, presmooth_solution_norm=0.0,
+                         presmooth_residual_norm=rn, presmooth_residual_ratio=1.0, restricted_rhs_norm=0.0,
+                         restricted_rhs_ratio=0.0, projector_norm=0.0, coarse_space_gap_norm=0.0,
+                         coarse_space_gap_ratio=0.0, coarse_correction_norm=xn, prolongated_correction_norm=xn,
+                         correction_alignment=0.0, corrected_residual_norm=resn,
+                         corrected_residual_vs_presmooth=_safe_ratio(resn, rn), correction_scale_raw=None,
+                         correction_scale_applied=1.0, postsmooth_solution_norm=xn, postsmooth_residual_norm=resn,
+                         postsmooth_residual_ratio=_safe_ratio(resn, rn), coarsest_mode=self.coarse_mode, notes="")
+            visits.append(_visit_record(visit))
+            return x
+        smooth = (lambda x: self.smooth_fine(x, rhs)) if lv == 0 else (lambda x: self.smooth_coarse(lv, x, rhs))
+        xs = smooth(np.zeros_like(rhs))
+        res = rhs - self.Alv(lv, xs)
+        presn = nrm(res)
+        rc = self.R[lv] @ res
+        proj = self.P[lv] @ rc
+        e = self._trace_level(lv + 1, rc, visits, counter, cyc)
+        Pe = self.P[lv] @ e
+        align = _alignment(res, Pe)
+        x, cres, raw, app, note1 = self.correction_decision(lv, xs, res, Pe)
+        crn = nrm(cres)
+        enrich = lv == 0 and self.enrich != "none"
+        enrich_note = f"root_enrichment:{self.enrich}" if enrich else ""
+        second, note2 = None, ""
+        if cyc == "w" or enrich:
+            rc2 = self.enrichment_rhs(cres) if enrich else self.R[lv] @ cres
+            e2 = self._trace_level(lv + 1, rc2, visits, counter, cyc)
+            Pe2 = self.P[lv] @ e2
+            align2 = _alignment(cres, Pe2)
+            x, cres2, raw2, app2, note2 = self.correction_decision(lv, x, cres, Pe2)
+            cr2n = nrm(cres2)
+            second = dict(second_restricted_rhs_norm=nrm(rc2), second_coarse_correction_norm=nrm(e2),
+                          second_prolongated_correction_norm=nrm(Pe2), second_correction_alignment=align2,
+                          second_correction_scale_raw=raw2, second_correction_scale_applied=app2,
+                          second_corrected_residual_norm=cr2n,
+                          second_corrected_residual_vs_corrected=_safe_ratio(cr2n, crn))
+        # the V-cycle record reports the residual after its (enrichment) second
+        # correction as corrected_residual_norm (multigrid_v4.py:1516-1563);
+        # the W-cycle record keeps the first (:1670-1712)
+        if second is not None and cyc == "v":
+            crn = second["second_corrected_residual_norm"]
+        extra = ""
+        x = smooth(x)
+        if lv == 0 and self.high:
+            x = smooth(x)
+            extra = "extra_fine_postsmooth"
+        postn = nrm(rhs - self.Alv(lv, x))
+        visit.update(is_coarsest=False, n_coarse_corrections=1 if second is None else 2,
+                     presmooth_solution_norm=nrm(xs), presmooth_residual_norm=presn,
+                     presmooth_residual_ratio=_safe_ratio(presn, rn), restricted_rhs_norm=nrm(rc),
+                     restricted_rhs_ratio=_safe_ratio(nrm(rc), presn), projector_norm=nrm(proj),
+                     coarse_space_gap_norm=nrm(res - proj), coarse_space_gap_ratio=_safe_ratio(nrm(res - proj), presn),
+                     coarse_correction_norm=nrm(e), prolongated_correction_norm=nrm(Pe), correction_alignment=align,
+                     correction_scale_raw=raw, correction_scale_applied=app, corrected_residual_norm=crn,
+                     corrected_residual_vs_presmooth=_safe_ratio(crn, presn), postsmooth_solution_norm=nrm(x),
+                     postsmooth_residual_norm=postn, postsmooth_residual_ratio=_safe_ratio(postn, rn),
+                     coarsest_mode="",
+                     notes=_merge_notes(note1, note2, enrich_note, extra))
+        if second is not None:
+            visit.update(second)
+        visits.append(_visit_record(visit))
+        return x
+
+
+# MultigridCycleVisit fields in declaration order (multigrid_v4.py:39-74)
+VISIT_FIELDS = (
+    "visit_id", "level", "cycle_type", "is_coarsest", "n_coarse_corrections", "rhs_norm", "jacobi_action_norm",
+    "presmooth_solution_norm", "presmooth_residual_norm", "presmooth_residual_ratio", "restricted_rhs_norm",
+    "restricted_rhs_ratio", "projector_norm", "coarse_space_gap_norm", "coarse_space_gap_ratio",
+    "coarse_correction_norm", "prolongated_correction_norm", "correction_alignment", "corrected_residual_norm",
+    "corrected_residual_vs_presmooth", "correction_scale_raw", "correction_scale_applied",
+    "second_restricted_rhs_norm", "second_coarse_correction_norm", "second_prolongated_correction_norm",
+    "second_correction_alignment", "second_correction_scale_raw", "second_correction_scale_applied",
+    "second_corrected_residual_norm", "second_corrected_residual_vs_corrected", "postsmooth_solution_norm",
+    "postsmooth_residual_norm", "postsmooth_residual_ratio", "coarsest_mode", "notes",
+)
+
+
+def _visit_record(v: dict) -> dict:
+    return {k: v.get(k) for k in VISIT_FIELDS}
+
+
+def _safe_ratio(num: float, den: float) -> float:
+    """multigrid_v4.py:840-843."""
+    if abs(den) <= 1e-300:
+        return 0.0 if abs(num) <= 1e-300 else float("inf")
+    return float(num / den)
+
+
+def _alignment(ref, corr) -> float:
+    """Cosine of the angle between a residual and a correction (multigrid_v4.py:855-862)."""
+    rn, cn = float(np.linalg.norm(ref)), float(np.linalg.norm(corr))
+    if rn <= 1e-300 or cn <= 1e-300:
+        return 0.0
+    return float(np.dot(ref, corr) / (rn * cn))
+
+
+def _merge_notes(*notes: str) -> str:
+    return "|".join(n for n in notes if n)
 
 
 def bf16_round(a32) -> np.ndarray:

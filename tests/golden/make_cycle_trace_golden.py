@@ -1,0 +1,64 @@
+"""Golden traces of one multigrid cycle from the reference's own ``cycle_trace``.
+
+Run from the repository root where the reference source tree is readable
+(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+
+    python tests/golden/make_cycle_trace_golden.py
+
+``GalerkinMatFreeGMG.cycle_trace`` (gpu_fem/multigrid_v4.py:1362-1728) runs
+unmodified on the host through the numpy-backed ``cupy`` stand-in in
+``_refshim.py``, on the inputs already committed in ``reference_small.npz``
+(the cant24 moduli ``E_hi`` / ``E_mid`` and right-hand side ``rhs``).  Each
+trace is written with the reference's own ``to_dict()`` into
+``cycle_trace_cant24.json``; the oracle's restatement (oracle/gmg.py) is
+pinned to it, and through the oracle the device trace.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import _refshim  # noqa: E402
+from make_golden import STACKS, _build  # noqa: E402
+
+TRACE_STACKS = {
+    "plain_cheb": STACKS["plain_cheb"],
+    "plain_jacobi": STACKS["plain_jacobi"],
+    "wcycle": STACKS["wcycle"],
+    "line_search": STACKS["line_search"],
+    "enrich": STACKS["enrich"],
+    "enrich_void": STACKS["enrich_void"],
+    "nb_line_search": STACKS["nb_line_search"],
+    "canonical": STACKS["canonical"],
+    "level_fp32": STACKS["level_fp32"],
+    "wcycle_enrich": dict(cycle_type="w", coarse_correction_policy="residual_line_search",
+                          root_enrichment_mode="void_gap_second"),
+}
+
+
+def main() -> None:
+    presets = _refshim.load("presets")
+    spec = presets.get_preset("cantilever_3d")
+    fx = np.load(os.path.join(HERE, "reference_small.npz"))
+    rhs = fx["cant24/rhs"]
+    out = {"case": "cant24", "n_levels": 3, "traces": {}}
+    for sname, stack in TRACE_STACKS.items():
+        for tag in ("hi", "mid"):
+            _, _, _, _, gmg = _build(spec, 3, stack)
+            gmg.setup(fx[f"cant24/E_{tag}"])
+            tr = gmg.cycle_trace(rhs).to_dict()
+            out["traces"][f"{sname}/{tag}"] = {"stack": stack, "trace": tr}
+    path = os.path.join(HERE, "cycle_trace_cant24.json")
+    with open(path, "w") as fh:
+        json.dump(out, fh, indent=0, sort_keys=True)
+    print(f"wrote {path}: {len(out['traces'])} traces")
+
+
+if __name__ == "__main__":
+    main()

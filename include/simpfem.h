@@ -160,6 +160,39 @@ int simpfem_gmg_destroy(simpfem_gmg* g);
 int simpfem_gmg_setup(simpfem_gmg* g, const double* E, const double* fine_diag_free, void* stream);
 /* z = M(rhs) (GalerkinMatFreeGMG.apply, multigrid_v4.py:1759-1767); FP64 free layout. */
 int simpfem_gmg_apply(simpfem_gmg* g, const double* rhs_free, double* z_free, void* stream);
+/* One base cycle traced on the device, then the root-local correction
+ * (GalerkinMatFreeGMG.cycle_trace, multigrid_v4.py:1362-1728; the inner Krylov
+ * wrapper is not traced).  rhs_free: device FP64 free layout.  cycle_type: 0 V,
+ * 1 W, -1 the hierarchy's own.  visits / summary: HOST arrays.  Each visit is
+ * SIMPFEM_TRACE_VISIT_LEN doubles in visit (pre-)order, NaN where the reference
+ * records None:
+ *   0 visit_id  1 level  2 is_coarsest  3 n_coarse_corrections  4 rhs_norm
+ *   5 jacobi_action_norm  6 presmooth_solution_norm  7 presmooth_residual_norm
+ *   8 restricted_rhs_norm  9 projector_norm  10 coarse_space_gap_norm
+ *   11 coarse_correction_norm  12 prolongated_correction_norm  13 correction_alignment
+ *   14 correction_scale_raw  15 correction_scale_applied  16 corrected_residual_norm
+ *   17 residual norm after the first correction  18 second_restricted_rhs_norm
+ *   19 second_coarse_correction_norm  20 second_prolongated_correction_norm
+ *   21 second_correction_alignment  22 second_correction_scale_raw
+ *   23 second_correction_scale_applied  24 second_corrected_residual_norm
+ *   25 postsmooth_solution_norm  26 postsmooth_residual_norm
+ *   27 first note, 28 second note (-1 none): 0 "", 1 degenerate_correction,
+ *      2 rejected_correction, 3 nonpositive_correction_scale, 4 clipped_correction_scale
+ *   29 root enrichment applied  30 extra fine post-smoothing
+ *   31 coarsest mode (-1 not the coarsest, 0 none, 1 dense, 2 iterative)
+ * summary (SIMPFEM_TRACE_SUMMARY_LEN doubles): 0 rhs_norm  1 jacobi_action_norm
+ *   2 output_norm  3 rz  4 output_residual_norm  5 residual norm before the
+ *   root-local correction  6 root-local raw scale  7 root-local applied scale
+ *   8 root-local note (0 "", 1 degenerate_root_local_correction,
+ *   2 rejected_root_local_inner_fgmres, 3 root_local_inner_fgmres,
+ *   4 nonpositive_root_local_scale, 5 clipped_root_local_scale)  9 contrast ratio
+ *   10 high contrast  11 fine degree  12 coarse sweeps  13 visits taken
+ *   14 coarsest mode.  *n_visits = visits taken (records beyond max_visits are
+ *   not written).  Synchronises the stream at every norm. */
+#define SIMPFEM_TRACE_VISIT_LEN 32
+#define SIMPFEM_TRACE_SUMMARY_LEN 16
+int simpfem_gmg_cycle_trace(simpfem_gmg* g, const double* rhs_free, int cycle_type, double* visits,
+                            int max_visits, int* n_visits, double* summary, void* stream);
 int simpfem_gmg_props_get(simpfem_gmg* g, simpfem_gmg_props* out);
 /* Average device time (ms) of one fused smoothing step of `level` (below the
  * coarsest) -- the operator kernel with the smoother's update fused into its

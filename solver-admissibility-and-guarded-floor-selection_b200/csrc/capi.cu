@@ -331,6 +331,26 @@ int simpfem_gmg_apply(simpfem_gmg* g, const double* rhs_free, double* z_free, vo
   SF_API_END
 }
 
+int simpfem_gmg_cycle_trace(simpfem_gmg* g, const double* rhs_free, int cycle_type, double* visits, int max_visits,
+                            int* n_visits, double* summary, void* stream) {
+  SF_API_BEGIN
+  if (!g || !rhs_free || !n_visits || !summary || max_visits < 0 || (max_visits > 0 && !visits))
+    throw InvalidArg{"simpfem_gmg_cycle_trace: invalid argument"};
+  if (cycle_type < -1 || cycle_type > 1) throw InvalidArg{"cycle_type must be 'v' or 'w'"};
+  Gmg& G = *g->impl;
+  if (!G.is_setup) throw NotSetup{"GalerkinMatFreeGMG.setup() must be called before cycle_trace()."};
+  Mesh& m = *G.m;
+  G.st = S(stream);
+  SF_CUDA(cudaMemsetAsync(g->bfull.p, 0, 8 * m.g.ndof, G.st));
+  SF_CUDA(launch_expand(F64, m.n_free, m.free_idx.as<int32_t>(), rhs_free, g->bfull.p, G.st));
+  std::vector<double> rec;
+  trace_cycle(G, g->bfull.as<double>(), cycle_type < 0 ? G.o.cycle_type : cycle_type, &rec, summary);
+  const int nv = (int)(rec.size() / kTraceVisitLen);
+  *n_visits = nv;
+  std::copy(rec.begin(), rec.begin() + (size_t)std::min(nv, max_visits) * kTraceVisitLen, visits);
+  SF_API_END
+}
+
 int simpfem_gmg_props_get(simpfem_gmg* g, simpfem_gmg_props* p) {
   SF_API_BEGIN
   if (!g || !p) throw InvalidArg{"simpfem_gmg_props_get: null argument"};

@@ -400,7 +400,7 @@ Gmg* gmg_create(Mesh* m, const simpfem_gmg_opts& o) {
 static const void* fine_E(Gmg& G, DType t) { return t == F64 ? G.E64.p : G.E32.p; }
 
 // level operator in the vector dtype vt, coefficient storage chosen by prec
-static void level_op(Gmg& G, int l, DType vt, int precsel, Epi epi, const void* u, EpiArgs ea) {
+void level_op(Gmg& G, int l, DType vt, int precsel, Epi epi, const void* u, EpiArgs ea) {
   ea.guard = G.guard;
   if (l == 0) {
     DType ft = vt;
@@ -425,7 +425,7 @@ static void level_op(Gmg& G, int l, DType vt, int precsel, Epi epi, const void* 
   SF_CUDA(launch_stencil(vt, ct, epi, L.g, coef, L.mask.as<uint8_t>(), u, ea, G.st));
 }
 
-static const void* level_dinv(Gmg& G, int l, DType t) {
+const void* level_dinv(Gmg& G, int l, DType t) {
   return t == F64 ? G.lv[l].dinv64.p : G.lv[l].dinv32.p;
 }
 
@@ -531,7 +531,7 @@ static void* run_smoother(Gmg& G, int l, DType t, int precsel, const void* rhs, 
 }
 
 // smooth at level l; x_in null => zero initial guess; result in one of lv[l].x
-static void* smooth(Gmg& G, int l, const void* rhs, const void* x_in) {
+void* smooth(Gmg& G, int l, const void* rhs, const void* x_in) {
   Level& L = G.lv[l];
   const int64_t n = L.g.ndof;
   double lm, lf = G.o.cheb_lower_frac;
@@ -572,7 +572,7 @@ static void* smooth(Gmg& G, int l, const void* rhs, const void* x_in) {
 // Coarsest solve (dense via explicit Cholesky inverse factor, or fixed Jacobi-PCG)
 static void fixed_pcg_coarse(Gmg& G, int l, const double* b, double* x);
 
-static void solve_coarsest(Gmg& G, const void* rhs, void* x) {
+void solve_coarsest(Gmg& G, const void* rhs, void* x) {
   const int l = G.L - 1;
   Level& L = G.lv[l];
   const int64_t n = L.g.ndof;
@@ -607,7 +607,7 @@ static void solve_coarsest(Gmg& G, const void* rhs, void* x) {
 // ----------------------------------------------------------------------------
 // Coarse correction at level l: x <- x + s c (line search) ; corrected residual
 // in `res_out` when non-null.
-static void coarse_correction(Gmg& G, int l, void* x, const void* res, const void* c, void* res_out) {
+void coarse_correction(Gmg& G, int l, void* x, const void* res, const void* c, void* res_out) {
   Level& L = G.lv[l];
   const int64_t n = L.g.ndof;
   const DType t = G.cyc;
@@ -645,7 +645,7 @@ static void coarse_correction(Gmg& G, int l, void* x, const void* res, const voi
 }
 
 // root enrichment right-hand side at level 0 (multigrid_v4.py:938-962)
-static void enrichment_rhs(Gmg& G, const void* residual, void* rc_out) {
+void enrichment_rhs(Gmg& G, const void* residual, void* rc_out) {
   Level& L0 = G.lv[0];
   Level& L1 = G.lv[1];
   const int64_t n = L0.g.ndof;
@@ -873,7 +873,7 @@ static void fgmres(Gmg& G, KrylovWs& K, const double* b, double* x, bool x0_zero
 
 // ----------------------------------------------------------------------------
 // root-local correction (multigrid_v4.py:964-1055)
-static void root_local(Gmg& G, const double* rhs, double* x) {
+void root_local(Gmg& G, const double* rhs, double* x) {
   Mesh& m = *G.m;
   const int64_t n = G.nfull();
   double* residual = G.tmp64a.as<double>();

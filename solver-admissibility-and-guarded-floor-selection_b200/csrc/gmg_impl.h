@@ -235,4 +235,26 @@ float time_smoother_step(Gmg& G, int l, int reps);
 void run_pcg(Gmg& G, const double* b, double* x, double tol, int maxiter, std::vector<double>* hist, int* iters,
              int* conv);
 
+// Building blocks of the cycle (vectors in the cycle dtype G.cyc, full layout of
+// the level), shared by the cycle itself and the traced cycle.
+// level operator: ea.y <- K_l u (EPI_APPLY) or ea.b - K_l u (EPI_RESID)
+void level_op(Gmg& G, int l, DType vt, int precsel, Epi epi, const void* u, EpiArgs ea);
+const void* level_dinv(Gmg& G, int l, DType t);
+// smoothing sweeps on level l from x_in (nullptr = zero); returns the buffer holding x
+void* smooth(Gmg& G, int l, const void* rhs, const void* x_in);
+void solve_coarsest(Gmg& G, const void* rhs, void* x);
+// x <- x + s c under the coarse-correction policy; the corrected residual in
+// res_out when non-null; the decision scalars stay in G.sc[0..8]
+void coarse_correction(Gmg& G, int l, void* x, const void* res, const void* c, void* res_out);
+void enrichment_rhs(Gmg& G, const void* residual, void* rc_out);
+// root-local correction of the FP64 full-layout x; decision scalars in G.sc[16..24]
+void root_local(Gmg& G, const double* rhs, double* x);
+
+// One cycle traced on the device (gpu_fem/multigrid_v4.py:1362-1728): records of
+// kTraceVisitLen doubles per visit in pre-order, and a kTraceSummaryLen summary.
+constexpr int kTraceVisitLen = 32;
+constexpr int kTraceSummaryLen = 16;
+void trace_cycle(Gmg& G, const double* rhs_full, int cycle_type, std::vector<double>* visits,
+                 double* summary);
+
 }  // namespace simpfem

@@ -73,7 +73,7 @@ struct RedWork {
 };
 
 // Multi-dot: out[k] = sum_i term_k(i), double accumulation, fixed order.
-//   mode 0: a*b ; mode 1: (a*c)*b ; mode 2: a*(b/c) where c != 0
+//   mode 0: a*b ; mode 1: (a*c)*b ; mode 2: a*(b/c) where c != 0 ; mode 3: (a*c)*(b*c)
 struct DotSet {
   const void* a[4] = {nullptr, nullptr, nullptr, nullptr};
   const void* b[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -79,6 +79,7 @@ __device__ __forceinline__ double dot_term(const DotSet& ds, int k, int64_t i) {
   if (ds.mode[k] == 0) return (double)a * (double)b;
   const T c = ((const T*)ds.c[k])[i];
   if (ds.mode[k] == 1) return (double)mul_rn(a, c) * (double)b;  // (a * c) * b
+  if (ds.mode[k] == 3) return (double)mul_rn(a, c) * (double)mul_rn(b, c);  // (a * c) * (b * c)
   // mode 2: a * (b / c) on entries with c != 0
   return c != T(0) ? (double)a * (double)(b / c) : 0.0;
 }

@@ -107,6 +107,7 @@ _SIGS = {
     "simpfem_gmg_destroy": (_I, [_P]),
     "simpfem_gmg_setup": (_I, [_P, _P, _P, _P]),
     "simpfem_gmg_apply": (_I, [_P, _P, _P, _P]),
+    "simpfem_gmg_cycle_trace": (_I, [_P, _P, _I, _P, _I, _P, _P, _P]),
     "simpfem_gmg_props_get": (_I, [_P, _P]),
     "simpfem_gmg_reset_lambda_cache": (_I, [_P]),
     "simpfem_gmg_fine_E": (_I, [_P, _P]),

@@ -19,7 +19,7 @@ from __future__ import annotations
 
 import ctypes
 import math
-from dataclasses import dataclass
+from dataclasses import asdict, dataclass, field
 from typing import Callable, Optional
 
 import numpy as np
@@ -46,6 +46,178 @@ class MultigridLevelStats:
     n_free: int
     nnz: int
     estimated_vram_bytes: int
+
+
+_CC_NOTES = ("", "degenerate_correction", "rejected_correction", "nonpositive_correction_scale",
+             "clipped_correction_scale")
+_RL_NOTES = ("", "degenerate_root_local_correction", "rejected_root_local_inner_fgmres", "root_local_inner_fgmres",
+             "nonpositive_root_local_scale", "clipped_root_local_scale")
+_COARSE_MODES = ("none", "dense", "iterative")
+
+
+@dataclass
+class MultigridCycleVisit:
+    """One level visit of a traced cycle (multigrid_v4.py:39-78)."""
+
+    visit_id: int
+    level: int
+    cycle_type: str
+    is_coarsest: bool
+    n_coarse_corrections: int
+    rhs_norm: float
+    jacobi_action_norm: float
+    presmooth_solution_norm: float
+    presmooth_residual_norm: float
+    presmooth_residual_ratio: float
+    restricted_rhs_norm: float
+    restricted_rhs_ratio: float
+    projector_norm: float
+    coarse_space_gap_norm: float
+    coarse_space_gap_ratio: float
+    coarse_correction_norm: float
+    prolongated_correction_norm: float
+    correction_alignment: float
+    corrected_residual_norm: float
+    corrected_residual_vs_presmooth: float
+    correction_scale_raw: Optional[float] = None
+    correction_scale_applied: float = 1.0
+    second_restricted_rhs_norm: Optional[float] = None
+    second_coarse_correction_norm: Optional[float] = None
+    second_prolongated_correction_norm: Optional[float] = None
+    second_correction_alignment: Optional[float] = None
+    second_correction_scale_raw: Optional[float] = None
+    second_correction_scale_applied: Optional[float] = None
+    second_corrected_residual_norm: Optional[float] = None
+    second_corrected_residual_vs_corrected: Optional[float] = None
+    postsmooth_solution_norm: float = 0.0
+    postsmooth_residual_norm: float = 0.0
+    postsmooth_residual_ratio: float = 0.0
+    coarsest_mode: str = ""
+    notes: str = ""
+
+    def to_dict(self) -> dict:
+        return asdict(self)
+
+
+@dataclass
+class MultigridCycleTrace:
+    """A traced cycle and the root-local correction after it (multigrid_v4.py:80-113)."""
+
+    cycle_type: str
+    rhs_norm: float
+    jacobi_action_norm: float
+    output_norm: float
+    z_over_jacobi: float
+    rz: float
+    pd: bool
+    output_residual_norm: float
+    output_residual_ratio: float
+    contrast_ratio: float
+    is_high_contrast: bool
+    fine_degree_adapt: int
+    coarse_iters_adapt: int
+    coarse_correction_policy: str
+    coarse_correction_acceptance_ratio: float
+    coarse_correction_max_scale: float
+    root_enrichment_mode: str
+    root_enrichment_weight_floor: float
+    root_enrichment_weight_power: float
+    root_local_correction_mode: str
+    root_local_correction_inner_steps: int
+    root_local_correction_inner_restart: int
+    root_local_correction_raw_scale: Optional[float]
+    root_local_correction_applied_scale: float
+    root_local_correction_residual_ratio: float
+    inner_krylov_steps: int
+    inner_krylov_restart: int
+    visits: list = field(default_factory=list)
+
+    def to_dict(self) -> dict:
+        return asdict(self)
+
+
+def _safe_ratio(num: float, den: float) -> float:
+    """multigrid_v4.py:840-843."""
+    if abs(den) <= 1e-300:
+        return 0.0 if abs(num) <= 1e-300 else float("inf")
+    return float(num / den)
+
+
+def _opt(v) -> Optional[float]:
+    return None if v is None or math.isnan(v) else float(v)
+
+
+def trace_from_records(visits, summary, cycle_type: str, options: dict) -> MultigridCycleTrace:
+    """Build the trace from the library's records (layout in include/simpfem.h,
+    simpfem_gmg_cycle_trace): ratios, notes and None fields follow
+    multigrid_v4.py:1362-1728.  ``options`` holds the hierarchy's constructor
+    settings echoed by the trace (coarse_correction_policy, ...)."""
+    out = []
+    for r in np.asarray(visits, dtype=np.float64).reshape(-1, 32):
+        coarsest = bool(r[2])
+        rn, presn, crn1 = float(r[4]), float(r[7]), float(r[17])
+        second = not coarsest and int(r[3]) == 2
+        notes = []
+        if not coarsest:
+            notes.append(_CC_NOTES[int(r[27])])
+            if second:
+                notes.append(_CC_NOTES[int(r[28])])
+            if r[29]:
+                notes.append(f"root_enrichment:{options['root_enrichment_mode']}")
+            if r[30]:
+                notes.append("extra_fine_postsmooth")
+        out.append(MultigridCycleVisit(
+            visit_id=int(r[0]), level=int(r[1]), cycle_type=cycle_type, is_coarsest=coarsest,
+            n_coarse_corrections=int(r[3]), rhs_norm=rn, jacobi_action_norm=float(r[5]),
+            presmooth_solution_norm=float(r[6]), presmooth_residual_norm=presn,
+            presmooth_residual_ratio=1.0 if coarsest else _safe_ratio(presn, rn),
+            restricted_rhs_norm=float(r[8]), restricted_rhs_ratio=0.0 if coarsest else _safe_ratio(r[8], presn),
+            projector_norm=float(r[9]), coarse_space_gap_norm=float(r[10]),
+            coarse_space_gap_ratio=0.0 if coarsest else _safe_ratio(r[10], presn),
+            coarse_correction_norm=float(r[11]), prolongated_correction_norm=float(r[12]),
+            correction_alignment=float(r[13]), corrected_residual_norm=float(r[16]),
+            corrected_residual_vs_presmooth=_safe_ratio(r[16], presn),
+            correction_scale_raw=_opt(r[14]), correction_scale_applied=float(r[15]),
+            second_restricted_rhs_norm=_opt(r[18]) if second else None,
+            second_coarse_correction_norm=_opt(r[19]) if second else None,
+            second_prolongated_correction_norm=_opt(r[20]) if second else None,
+            second_correction_alignment=_opt(r[21]) if second else None,
+            second_correction_scale_raw=_opt(r[22]) if second else None,
+            second_correction_scale_applied=_opt(r[23]) if second else None,
+            second_corrected_residual_norm=_opt(r[24]) if second else None,
+            second_corrected_residual_vs_corrected=_safe_ratio(r[24], crn1) if second else None,
+            postsmooth_solution_norm=float(r[25]), postsmooth_residual_norm=float(r[26]),
+            postsmooth_residual_ratio=_safe_ratio(r[26], rn),
+            coarsest_mode=_COARSE_MODES[int(r[31])] if coarsest else "",
+            notes="|".join(n for n in notes if n),
+        ))
+    s = np.asarray(summary, dtype=np.float64)
+    local_note = _RL_NOTES[int(s[8])]
+    if local_note:
+        root = next((v for v in out if v.level == 0 and not v.is_coarsest), None)
+        if root is not None:
+            root.notes = "|".join(n for n in (root.notes, local_note) if n)
+    rz = float(s[3])
+    return MultigridCycleTrace(
+        cycle_type=cycle_type, rhs_norm=float(s[0]), jacobi_action_norm=float(s[1]), output_norm=float(s[2]),
+        z_over_jacobi=_safe_ratio(s[2], s[1]), rz=rz, pd=bool(rz > 0.0), output_residual_norm=float(s[4]),
+        output_residual_ratio=_safe_ratio(s[4], s[0]), contrast_ratio=float(s[9]), is_high_contrast=bool(s[10]),
+        fine_degree_adapt=int(s[11]), coarse_iters_adapt=int(s[12]),
+        coarse_correction_policy=options["coarse_correction_policy"],
+        coarse_correction_acceptance_ratio=float(options["coarse_correction_acceptance_ratio"]),
+        coarse_correction_max_scale=float(options["coarse_correction_max_scale"]),
+        root_enrichment_mode=options["root_enrichment_mode"],
+        root_enrichment_weight_floor=float(options["root_enrichment_weight_floor"]),
+        root_enrichment_weight_power=float(options["root_enrichment_weight_power"]),
+        root_local_correction_mode=options["root_local_correction_mode"],
+        root_local_correction_inner_steps=int(options["root_local_correction_inner_steps"]),
+        root_local_correction_inner_restart=int(options["root_local_correction_inner_restart"]),
+        root_local_correction_raw_scale=_opt(s[6]), root_local_correction_applied_scale=float(s[7]),
+        root_local_correction_residual_ratio=_safe_ratio(s[4], s[5]),
+        inner_krylov_steps=int(options["inner_krylov_steps"]),
+        inner_krylov_restart=int(options["inner_krylov_restart"]),
+        visits=out,
+    )
 
 
 class GalerkinMatFreeGMG:
@@ -359,6 +531,41 @@ class GalerkinMatFreeGMG:
             "jacobi_norm": jn,
             "z_over_jacobi": zn / max(jn, 1e-30),
         }
+
+    def cycle_trace(self, rhs, *, cycle_type: Optional[str] = None) -> MultigridCycleTrace:
+        """Structured trace of one multigrid cycle on ``rhs`` (multigrid_v4.py:1362-1438):
+        the norms of every level visit, measured on the device between the
+        cycle's own kernels, then the root-local correction.  A diagnostic:
+        the library synchronises at every norm; the solve path is unchanged."""
+        if not self._is_setup:
+            raise RuntimeError("GalerkinMatFreeGMG.setup() must be called before cycle_trace().")
+        cycle = self._cycle_type if cycle_type is None else cycle_type
+        if cycle not in {"v", "w"}:
+            raise ValueError(f"cycle_type must be 'v' or 'w'; got {cycle!r}")
+        torch = _lib.require_cuda()
+        rhs64 = _lib.as_cuda(rhs, torch.float64)
+        cap = 2 ** self._n_levels
+        visits = np.full((cap, 32), np.nan)
+        summary = np.full(16, np.nan)
+        nv = ctypes.c_int()
+        _lib.call("simpfem_gmg_cycle_trace", self._h, _lib.ptr(rhs64), 0 if cycle == "v" else 1,
+                  visits.ctypes.data, cap, ctypes.byref(nv), summary.ctypes.data, _lib.stream_ptr())
+        if nv.value > cap:
+            raise RuntimeError(f"cycle_trace: {nv.value} visits exceed the record capacity {cap}")
+        options = {
+            "coarse_correction_policy": self._coarse_correction_policy,
+            "coarse_correction_acceptance_ratio": self._coarse_correction_acceptance_ratio,
+            "coarse_correction_max_scale": self._coarse_correction_max_scale,
+            "root_enrichment_mode": self._root_enrichment_mode,
+            "root_enrichment_weight_floor": self._root_enrichment_weight_floor,
+            "root_enrichment_weight_power": self._root_enrichment_weight_power,
+            "root_local_correction_mode": self._root_local_correction_mode,
+            "root_local_correction_inner_steps": self._root_local_correction_inner_steps,
+            "root_local_correction_inner_restart": self._root_local_correction_inner_restart,
+            "inner_krylov_steps": self._inner_krylov_steps,
+            "inner_krylov_restart": self._inner_krylov_restart,
+        }
+        return trace_from_records(visits[: nv.value], summary, cycle, options)
 
     def estimate_kappa_eff(self, n_iter: int = 30) -> float:
         """Lanczos estimate of kappa(M K) for a linear preconditioner

@@ -1,0 +1,78 @@
+"""GalerkinMatFreeGMG.cycle_trace on the device (csrc/trace.cu through
+simpfem_gmg_cycle_trace) against the reference's own traces
+(tests/golden/cycle_trace_cant24.json, to which the oracle is pinned): every
+visit and every field of 20 traces -- V and W cycles, line search, both
+enrichment families, both root-local corrections, FP32 coarse levels -- in
+the FP64 cycle, to 1e-9 relative (1e-6 with FP32 levels).  In the FP32 cycle
+the traced V-cycle's answer is the preconditioner's, and a trace leaves the
+hierarchy's apply unchanged."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from test_gpu_parity import _components
+from test_oracle_cycle_trace import assert_trace_close
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "cycle_trace_cant24.json")
+with open(GOLDEN) as _fh:
+    _TRACES = json.load(_fh)["traces"]
+
+
+@pytest.mark.parametrize("key", sorted(_TRACES))
+def test_device_trace_matches_reference(cuda, ref, key):
+    case = _TRACES[key]
+    _, gmg, _ = _components("cant24", case["stack"])
+    gmg.setup(cuda.as_tensor(ref[f"cant24/E_{key.split('/')[1]}"], device="cuda"))
+    got = gmg.cycle_trace(cuda.as_tensor(ref["cant24/rhs"], device="cuda")).to_dict()
+    rtol = 1e-6 if key.startswith("level_fp32") else 1e-9
+    assert_trace_close(got, case["trace"], rtol, key)
+
+
+def test_trace_cycle_type_override(cuda, ref):
+    _, gmg, _ = _components("cant24", {})
+    gmg.setup(cuda.as_tensor(ref["cant24/E_mid"], device="cuda"))
+    rhs = cuda.as_tensor(ref["cant24/rhs"], device="cuda")
+    assert_trace_close(gmg.cycle_trace(rhs, cycle_type="w").to_dict(), _TRACES["wcycle/mid"]["trace"], 1e-9, "w")
+    with pytest.raises(ValueError, match="cycle_type"):
+        gmg.cycle_trace(rhs, cycle_type="x")
+
+
+@pytest.mark.parametrize("cycle", ["v", "w"])
+def test_fp32_cycle_trace_four_levels(cuda, cycle):
+    import torch
+
+    from gpu_fem.paper4 import _build_components
+    from gpu_fem.presets import cantilever_spec
+
+    spec, _, _, _, _, F, _, gmg = _build_components(cantilever_spec(48, 24, 12), n_levels=4, cycle_type=cycle,
+                                                     cycle_precision="fp32")
+    nel = spec.nelx * spec.nely * spec.nelz
+    rng = np.random.default_rng(3)
+    E = torch.as_tensor(1e-3 + (1 - 1e-3) * (rng.random(nel) > 0.3), device="cuda")
+    gmg.setup(E)
+    z0 = gmg.apply(F)
+    tr = gmg.cycle_trace(F)
+    z1 = gmg.apply(F)
+    assert torch.equal(z0, z1)  # the trace leaves the hierarchy as it was
+    levels = [v.level for v in tr.visits]
+    if cycle == "v":
+        assert levels == [0, 1, 2, 3]
+        # same kernels in the same order as apply: the same answer
+        assert tr.output_norm == pytest.approx(float(torch.linalg.norm(z0)), rel=1e-12)
+        assert tr.rz == pytest.approx(float(torch.dot(F, z0)), rel=1e-12)
+    else:
+        assert len(levels) == 15 and levels[:4] == [0, 1, 2, 3]
+        # the W-cycle trace forms its second residual as res - A c (the cycle as rhs - A x)
+        assert tr.output_norm == pytest.approx(float(torch.linalg.norm(z0)), rel=1e-4)
+        scale = float(torch.linalg.norm(F)) * float(torch.linalg.norm(z0))
+        assert abs(tr.rz - float(torch.dot(F, z0))) <= 1e-4 * scale
+    assert [v.visit_id for v in tr.visits] == list(range(len(levels)))
+    assert tr.visits[-1].is_coarsest and tr.visits[-1].coarsest_mode == "dense"
+    assert all(np.isfinite(v.postsmooth_residual_norm) for v in tr.visits)
+    assert tr.pd == (tr.rz > 0.0)
+    assert tr.rhs_norm == pytest.approx(float(torch.linalg.norm(F)), rel=1e-12)

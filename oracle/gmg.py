@@ -340,6 +340,41 @@ class GMG:
             x = self.root_local(x, rhs - self.A0(x))
         return x
 
+    # ------------------------------------------------------------ diagnostics (:1057-1117, :1348-1360)
+    def probe_quality(self, rhs) -> dict:
+        """Preconditioner action against the Jacobi action on one right-hand side."""
+        rhs = np.asarray(rhs, dtype=np.float64)
+        z = self.apply(rhs)
+        zn, jn = float(np.linalg.norm(z)), float(np.linalg.norm(self.dinv[0] * rhs))
+        return {"finite": bool(np.all(np.isfinite(z))), "pd": float(rhs @ z) > 0.0, "z_norm": zn,
+                "jacobi_norm": jn, "z_over_jacobi": zn / max(jn, 1e-30)}
+
+    def estimate_kappa_eff(self, n_iter: int = 30) -> float:
+        """lambda_max / lambda_min (positive Ritz values) of n_iter Lanczos steps on
+        M K from numpy's RandomState(0) start vector."""
+        if (self.cc != "none" or self.enrich != "none" or self.rl != "none" or self.ik > 0):
+            raise RuntimeError("estimate_kappa_eff requires a linear preconditioner")
+        n = len(self.free[0])
+        v = np.random.RandomState(0).standard_normal(n)
+        v /= np.linalg.norm(v)
+        alpha, beta = np.zeros(n_iter), np.zeros(max(n_iter - 1, 0))
+        v_prev = np.zeros(n)
+        for j in range(n_iter):
+            w = self.apply(self.A0(v))
+            alpha[j] = float(v @ w)
+            w = w - alpha[j] * v
+            if j > 0:
+                w = w - beta[j - 1] * v_prev
+            if j < n_iter - 1:
+                beta[j] = float(np.linalg.norm(w))
+                if beta[j] < 1e-14:
+                    alpha, beta = alpha[: j + 1], beta[:j]
+                    break
+                v_prev, v = v, w / beta[j]
+        eigs = np.linalg.eigvalsh(np.diag(alpha) + np.diag(beta, 1) + np.diag(beta, -1))
+        eigs = eigs[eigs > 0]
+        return float("nan") if len(eigs) == 0 else float(eigs[-1] / max(eigs[0], 1e-300))
+
     # ------------------------------------------------------------ cycle trace (:1362-1728)
     def cycle_trace(self, rhs, cycle_type=None) -> dict:
         """One traced base cycle, then the root-local correction: the dictionary

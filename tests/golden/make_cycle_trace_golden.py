@@ -11,7 +11,10 @@ unmodified on the host through the numpy-backed ``cupy`` stand-in in
 (the cant24 moduli ``E_hi`` / ``E_mid`` and right-hand side ``rhs``).  Each
 trace is written with the reference's own ``to_dict()`` into
 ``cycle_trace_cant24.json``; the oracle's restatement (oracle/gmg.py) is
-pinned to it, and through the oracle the device trace.
+pinned to it, and through the oracle the device trace.  The same file holds
+the two other diagnostics of the hierarchy, ``probe_quality`` (:1348-1360) and
+``estimate_kappa_eff`` (:1057-1117), for the linear stacks; the Lanczos start
+vector is the stand-in's ``RandomState(0).standard_normal`` (numpy's generator).
 """
 
 from __future__ import annotations
@@ -54,6 +57,15 @@ def main() -> None:
             gmg.setup(fx[f"cant24/E_{tag}"])
             tr = gmg.cycle_trace(rhs).to_dict()
             out["traces"][f"{sname}/{tag}"] = {"stack": stack, "trace": tr}
+    out["diagnostics"] = {}
+    for sname in ("plain_cheb", "plain_jacobi", "wcycle", "level_fp32"):
+        for tag in ("hi", "mid"):
+            _, _, _, _, gmg = _build(spec, 3, TRACE_STACKS[sname])
+            gmg.setup(fx[f"cant24/E_{tag}"])
+            pq = gmg.probe_quality(rhs)
+            kappa = gmg.estimate_kappa_eff(30)
+            out["diagnostics"][f"{sname}/{tag}"] = {"stack": TRACE_STACKS[sname], "probe_quality": pq,
+                                                    "kappa_eff_30": kappa}
     path = os.path.join(HERE, "cycle_trace_cant24.json")
     with open(path, "w") as fh:
         json.dump(out, fh, indent=0, sort_keys=True)

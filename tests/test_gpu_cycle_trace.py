@@ -76,3 +76,27 @@ def test_fp32_cycle_trace_four_levels(cuda, cycle):
     assert all(np.isfinite(v.postsmooth_residual_norm) for v in tr.visits)
     assert tr.pd == (tr.rz > 0.0)
     assert tr.rhs_norm == pytest.approx(float(torch.linalg.norm(F)), rel=1e-12)
+
+
+with open(GOLDEN) as _fh:
+    _DIAG = json.load(_fh)["diagnostics"]
+
+
+@pytest.mark.parametrize("key", sorted(_DIAG))
+def test_device_probe_quality_and_kappa_match_reference(cuda, ref, key):
+    """probe_quality (multigrid_v4.py:1348-1360) and the 30-step Lanczos
+    estimate_kappa_eff (:1057-1117) of the device hierarchy against the
+    reference's values on the same start vector."""
+    case = _DIAG[key]
+    _, gmg, _ = _components("cant24", case["stack"])
+    gmg.setup(cuda.as_tensor(ref[f"cant24/E_{key.split('/')[1]}"], device="cuda"))
+    pq = gmg.probe_quality(cuda.as_tensor(ref["cant24/rhs"], device="cuda"))
+    want = case["probe_quality"]
+    assert pq["finite"] == want["finite"] and pq["pd"] == want["pd"]
+    rtol = 1e-6 if key.startswith("level_fp32") else 1e-9
+    for k in ("z_norm", "jacobi_norm", "z_over_jacobi"):
+        assert pq[k] == pytest.approx(want[k], rel=rtol), k
+    # Lanczos amplifies the FP32 levels' rounding (FP32 vs FP64 levels differ by 3e-5 here)
+    ktol = 1e-5 if key.startswith("level_fp32") else 1e-7
+    assert gmg.estimate_kappa_eff(30) == pytest.approx(case["kappa_eff_30"], rel=ktol)
+    assert gmg.kappa_eff == pytest.approx(case["kappa_eff_30"], rel=ktol)

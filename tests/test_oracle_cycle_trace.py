@@ -92,3 +92,21 @@ def test_trace_rejects_unknown_cycle_and_missing_setup(ref):
     g.setup(ref["cant24/E_mid"])
     with pytest.raises(ValueError, match="cycle_type"):
         g.cycle_trace(ref["cant24/rhs"], cycle_type="f")
+
+
+def _diagnostics():
+    return sorted(_load()["diagnostics"])
+
+
+@pytest.mark.parametrize("key", _diagnostics())
+def test_oracle_probe_quality_and_kappa_match_reference(ref, key):
+    case = _load()["diagnostics"][key]
+    op = S.Operator(24, 12, 6, ref["cant24/free"])
+    g = GMG(op, n_levels=3, **dict(dict(fine_smoother="fp64"), **case["stack"]))
+    g.setup(ref[f"cant24/E_{key.split('/')[1]}"])
+    pq = g.probe_quality(ref["cant24/rhs"])
+    want = case["probe_quality"]
+    assert pq["finite"] == want["finite"] and pq["pd"] == want["pd"]
+    for k in ("z_norm", "jacobi_norm", "z_over_jacobi"):
+        assert pq[k] == pytest.approx(want[k], rel=1e-9), k
+    assert g.estimate_kappa_eff(30) == pytest.approx(case["kappa_eff_30"], rel=1e-8)

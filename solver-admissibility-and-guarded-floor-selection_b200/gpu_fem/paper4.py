@@ -66,3 +66,37 @@ PLAIN_JACOBI_STACK = dict(
     fine_smoother="fp64", smoother_type="jacobi", cycle_type="v",
     coarse_correction_policy="none", root_local_correction_mode="none", inner_krylov_steps=0,
 )
+
+
+# ---------------------------------------------------------------------------
+# Moduli fields and Krylov entry points of the same runner (run_experiments_e1_e10.py:182-219),
+# used by the phase-5 pathology driver.
+def _E_e(spec, rho_scalar: float = 0.5, penal: float = 3.0, E0=1.0, Emin=1e-9):
+    """Uniform-density SIMP moduli Emin + (E0 - Emin) rho^penal on the device."""
+    torch = _lib.require_cuda()
+    n = spec.nelx * spec.nely * spec.nelz
+    rho = torch.full((n,), float(rho_scalar), dtype=torch.float64, device="cuda")
+    return Emin + (E0 - Emin) * rho ** penal
+
+
+def _E_e_heterogeneous(spec, volfrac: float = 0.5, penal: float = 3.0, rho_min: float = 0.01,
+                       rho_max: float = 1.0, seed: int = 0, E0: float = 1.0, Emin: float = 1e-9):
+    """Binary-contrast field: each element rho_max with probability volfrac
+    (numpy default_rng(seed)), rho_min otherwise; moduli Emin + (E0 - Emin) rho^penal."""
+    torch = _lib.require_cuda()
+    n = spec.nelx * spec.nely * spec.nelz
+    rng = np.random.default_rng(seed)
+    rho = torch.as_tensor(np.where(rng.random(n) < volfrac, rho_max, rho_min).astype(np.float64), device="cuda")
+    return Emin + (E0 - Emin) * rho ** penal
+
+
+def _pcg(A_op, b, M_op, tol=1e-6, maxiter=200, history=None):
+    from .solver_v2 import _cupy_pcg
+
+    return _cupy_pcg(A_op, b, M_op, tol=tol, maxiter=maxiter, history=history)
+
+
+def _fgmres(A_op, b, M_op, tol=1e-6, maxiter=200, restart=32, history=None):
+    from .multigrid_v4 import _cupy_fgmres
+
+    return _cupy_fgmres(A_op, b, M_op, tol=tol, maxiter=maxiter, restart=restart, history=history)

@@ -503,11 +503,64 @@ cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n
   return sf_launched(2);
 }
 
+// The FP32 copy with 16-byte row starts (n % 4 == 0): one warp per row, the
+// row read as float4 with eight of them per lane in flight, so the longest
+// rows (n / 128 float4 per lane) take a few memory round trips instead of one
+// per 128 entries.  The diagonal-aligned start of an upper row and the row's
+// end are read as scalars.  FP64 accumulation in a fixed order per row.
+__device__ __forceinline__ double dot4(float4 a, double2 b0, double2 b1) {
+  return ((double)a.x * b0.x + (double)a.y * b0.y) + ((double)a.z * b1.x + (double)a.w * b1.y);
+}
+
+template <int UPPER>
+__global__ void __launch_bounds__(256) tri_matvec_f32v_kernel(const float* __restrict__ M, int n,
+                                                              const double* __restrict__ b,
+                                                              double* __restrict__ y, const int* guard) {
+  if (guard_off(guard)) return;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float* r = M + (int64_t)row * n;
+  const int lo = UPPER ? row : 0, hi = UPPER ? n : row + 1;
+  const int lo4 = min(hi, (lo + 3) & ~3);  // first column of the float4 body
+  const int nv = (hi - lo4) >> 2;          // float4 in the body
+  const int t0 = lo4 + 4 * nv;             // first column of the scalar tail
+  double acc[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) acc[u] = 0.0;
+  if (lane < lo4 - lo) acc[0] += (double)r[lo + lane] * b[lo + lane];
+  if (lane < hi - t0) acc[1] += (double)r[t0 + lane] * b[t0 + lane];
+  const float4* r4 = reinterpret_cast<const float4*>(r + lo4);
+  const double2* b2 = reinterpret_cast<const double2*>(b + lo4);
+  int v = lane;
+  for (; v + 224 < nv; v += 256) {
+    float4 a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] = __ldg(r4 + v + 32 * u);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int q = v + 32 * u;
+      acc[u] += dot4(a[u], __ldg(b2 + 2 * q), __ldg(b2 + 2 * q + 1));
+    }
+  }
+  for (; v < nv; v += 32) acc[2] += dot4(__ldg(r4 + v), __ldg(b2 + 2 * v), __ldg(b2 + 2 * v + 1));
+  double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  s = warp_sum(s);
+  if (lane == 0) y[row] = s;
+}
+
 cudaError_t launch_coarsest_solve_f32(const float* Linv, const float* LinvT, int n, const double* b, double* tmp,
                                       double* x, const int* guard, cudaStream_t s) {
   const int blocks = div_up((int64_t)n * 32, 256);
-  tri_matvec_kernel<0, float><<<blocks, 256, 0, s>>>(Linv, n, b, tmp, guard);
-  tri_matvec_kernel<1, float><<<blocks, 256, 0, s>>>(LinvT, n, tmp, x, guard);
+  const bool vec = n % 4 == 0 && ((uintptr_t)Linv & 15) == 0 && ((uintptr_t)LinvT & 15) == 0 &&
+                   ((uintptr_t)b & 15) == 0 && ((uintptr_t)tmp & 15) == 0;
+  if (vec) {
+    tri_matvec_f32v_kernel<0><<<blocks, 256, 0, s>>>(Linv, n, b, tmp, guard);
+    tri_matvec_f32v_kernel<1><<<blocks, 256, 0, s>>>(LinvT, n, tmp, x, guard);
+  } else {
+    tri_matvec_kernel<0, float><<<blocks, 256, 0, s>>>(Linv, n, b, tmp, guard);
+    tri_matvec_kernel<1, float><<<blocks, 256, 0, s>>>(LinvT, n, tmp, x, guard);
+  }
   return sf_launched(2);
 }
 

@@ -130,7 +130,10 @@ typedef struct simpfem_gmg_opts {
                                       smoother precision; SIMPFEM_F32: mixed mode, the whole
                                       V-cycle in FP32 with BF16-stored coarse stencils
                                       (no reference counterpart) */
-  int use_graphs;                  /* capture the preconditioner apply in a CUDA graph */
+  int use_graphs;                  /* 1: the V/W-cycle body is captured as a CUDA graph on the
+                                      second cycle after each setup (per skip-flag pointer) and
+                                      replayed after that; identical kernels and arguments.
+                                      0 (the C default): every kernel launched directly */
 } simpfem_gmg_opts;
 
 void simpfem_gmg_default_opts(simpfem_gmg_opts* o);
@@ -152,6 +155,7 @@ typedef struct simpfem_gmg_props {
   int coarse_regularised;   /* 1 if the eps-regularised retry was used */
   int lambda_reestimated;   /* 1 if the last setup re-estimated lambda_max */
   int64_t nnz[8];           /* structural nonzeros of the coarse operators (free-free) */
+  int64_t cycle_graph_replays; /* cycles run by replaying a captured graph (use_graphs) */
 } simpfem_gmg_props;
 
 int simpfem_gmg_create(simpfem_mesh* m, const simpfem_gmg_opts* opts, simpfem_gmg** out);

@@ -374,6 +374,7 @@ int simpfem_gmg_props_get(simpfem_gmg* g, simpfem_gmg_props* p) {
   p->coarse_mode = G.coarse_mode;
   p->coarse_regularised = G.coarse_reg ? 1 : 0;
   p->lambda_reestimated = G.lam_reest ? 1 : 0;
+  p->cycle_graph_replays = G.graph_replays;
   SF_API_END
 }
 

@@ -742,13 +742,105 @@ static void* cycle(Gmg& G, int l, const void* rhs) {
   return x;
 }
 
-// base cycle in FP64 (rhs64 -> out64)
+// kernel nodes of a captured graph
+static int kernel_nodes(cudaGraph_t graph) {
+  size_t nn = 0;
+  SF_CUDA(cudaGraphGetNodes(graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) SF_CUDA(cudaGraphGetNodes(graph, nodes.data(), &nn));
+  int k = 0;
+  for (cudaGraphNode_t v : nodes) {
+    cudaGraphNodeType t;
+    SF_CUDA(cudaGraphNodeGetType(v, &t));
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
+// The cycle body on the fixed cycle-dtype input `in` (cyc_in, or rhs64 in the
+// FP64 cycle): run directly, or captured once per setup and guard pointer on a
+// private stream and replayed on the hierarchy's stream (Gmg::CycleGraph).
+// Replays run the identical kernels with identical arguments.
+static void* run_cycle(Gmg& G, const void* in) {
+  if (!G.o.use_graphs || G.graphs_off) return cycle(G, 0, in);
+  Gmg::CycleGraph* cg = nullptr;
+  for (Gmg::CycleGraph& c : G.graphs)
+    if (c.guard == G.guard) cg = &c;
+  if (!cg) {
+    G.graphs.emplace_back();
+    cg = &G.graphs.back();
+    cg->guard = G.guard;
+  }
+  if (cg->epoch != G.setup_epoch) {
+    cg->epoch = G.setup_epoch;
+    cg->valid = false;
+    cg->direct = 0;
+  }
+  if (cg->valid) {
+    SF_CUDA(cudaGraphLaunch(cg->exec, G.st));
+    SF_CUDA(sf_launched(cg->launches));
+    ++G.graph_replays;
+    return cg->out;
+  }
+  if (cg->direct++ == 0) return cycle(G, 0, in);  // first cycle after a setup: direct
+  if (!G.cap_stream) SF_CUDA(cudaStreamCreateWithFlags(&G.cap_stream, cudaStreamNonBlocking));
+  cudaStream_t user = G.st;
+  cudaGraph_t graph = nullptr;
+  void* out = nullptr;
+  bool ok = cudaStreamBeginCapture(G.cap_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    G.st = G.cap_stream;
+    try {
+      out = cycle(G, 0, in);
+    } catch (...) {  // the stream must leave capture mode before anything is reported
+      ok = false;
+    }
+    G.st = user;
+    ok = (cudaStreamEndCapture(G.cap_stream, &graph) == cudaSuccess) && ok && graph != nullptr;
+  }
+  int nk = 0;
+  if (ok) {
+    nk = kernel_nodes(graph);
+    sf_launched(-nk);  // captured, not run
+    if (cg->exec) {  // the previous setup's executable, when the topology is unchanged
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(cg->exec, graph, &info) != cudaSuccess) {
+        cudaGraphExecDestroy(cg->exec);
+        cg->exec = nullptr;
+      }
+    }
+    if (!cg->exec && cudaGraphInstantiate(&cg->exec, graph, 0) != cudaSuccess) {
+      cg->exec = nullptr;
+      ok = false;
+    }
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();  // a refused capture leaves its error here; the cycle then runs directly
+  if (!ok) {
+    G.graphs_off = true;
+    return cycle(G, 0, in);
+  }
+  cg->launches = nk;
+  cg->out = out;
+  cg->valid = true;
+  SF_CUDA(cudaGraphLaunch(cg->exec, G.st));
+  SF_CUDA(sf_launched(nk));
+  ++G.graph_replays;
+  return out;
+}
+
+// base cycle in FP64 (rhs -> out)
 static void base_cycle(Gmg& G, const double* rhs, double* out) {
   const int64_t n = G.nfull();
   if (G.cyc == F32) {
     SF_CUDA(launch_convert(F64, F32, rhs, G.cyc_in.p, n, G.guard, G.st));
-    void* r = cycle(G, 0, G.cyc_in.p);
+    void* r = run_cycle(G, G.cyc_in.p);
     SF_CUDA(launch_convert(F32, F64, r, out, n, G.guard, G.st));
+  } else if (G.o.use_graphs && !G.graphs_off) {
+    // a captured cycle reads a fixed input buffer
+    SF_CUDA(launch_copy(F64, n, rhs, G.rhs64.p, G.guard, G.st));
+    void* r = run_cycle(G, G.rhs64.p);
+    SF_CUDA(launch_copy(F64, n, r, out, G.guard, G.st));
   } else {
     void* r = cycle(G, 0, rhs);
     SF_CUDA(launch_copy(F64, n, r, out, G.guard, G.st));
@@ -1174,6 +1266,7 @@ static void setup_coarsest(Gmg& G) {
 }
 
 void gmg_setup(Gmg& G, const double* E, const double* fine_diag_free) {
+  ++G.setup_epoch;  // captured cycles hold the previous setup's launch arguments
   Mesh& m = *G.m;
   const int64_t n = m.g.ndof;
   const int64_t ne = m.g.ne();

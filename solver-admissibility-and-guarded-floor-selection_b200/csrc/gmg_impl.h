@@ -203,6 +203,37 @@ struct Gmg {
   DevBuf hist_dev;
   PinnedBuf hist_pin;
 
+  // The V/W-cycle body captured as a CUDA graph (use_graphs): one per guard
+  // pointer (the kernels' skip flag is a launch argument), valid for the setup
+  // it was captured after -- every setup changes host-side launch arguments
+  // (Chebyshev coefficients, sweep counts) and bumps setup_epoch.  The first
+  // cycle after a setup runs directly, the second is captured (and replayed),
+  // later ones are replayed.  A capture that fails turns graphs off for the
+  // hierarchy.
+  struct CycleGraph {
+    const int* guard = nullptr;
+    void* out = nullptr;  // level-0 buffer holding the cycle's answer
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;    // kernel nodes (launch accounting)
+    uint64_t epoch = 0;  // setup the graph belongs to (0 = none)
+    bool valid = false;  // exec holds this epoch's cycle
+    int direct = 0;      // direct runs since that setup
+  };
+  std::vector<CycleGraph> graphs;
+  uint64_t setup_epoch = 0;
+  bool graphs_off = false;
+  int64_t graph_replays = 0;
+  cudaStream_t cap_stream = nullptr;  // private stream the cycle is captured on
+
+  Gmg() = default;
+  Gmg(const Gmg&) = delete;
+  Gmg& operator=(const Gmg&) = delete;
+  ~Gmg() {
+    for (CycleGraph& c : graphs)
+      if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+  }
+
   int64_t nfull() const { return m->g.ndof; }
 };
 

@@ -78,6 +78,7 @@ class GmgProps(ctypes.Structure):
         ("coarse_regularised", ctypes.c_int),
         ("lambda_reestimated", ctypes.c_int),
         ("nnz", ctypes.c_int64 * 8),
+        ("cycle_graph_replays", ctypes.c_int64),
     ]
 
 

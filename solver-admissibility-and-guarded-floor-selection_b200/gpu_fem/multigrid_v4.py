@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import os
 from dataclasses import asdict, dataclass, field
 from typing import Callable, Optional
 
@@ -256,6 +257,7 @@ class GalerkinMatFreeGMG:
         inner_krylov_steps: int = 0,
         inner_krylov_restart: Optional[int] = None,
         cycle_precision: str = "fp64",
+        use_graphs: Optional[bool] = None,
     ) -> None:
         if smoother_type not in {"chebyshev", "jacobi"}:
             raise ValueError(f"smoother_type must be 'chebyshev' or 'jacobi'; got {smoother_type!r}")
@@ -380,6 +382,13 @@ class GalerkinMatFreeGMG:
         o.inner_krylov_steps = int(inner_krylov_steps)
         o.inner_krylov_restart = self._inner_krylov_restart
         o.cycle_precision = _lib.F32 if cycle_precision == "fp32" else _lib.F64
+        # the cycle body captured once per setup as a CUDA graph and replayed;
+        # off unless asked for (use_graphs=True or SIMPFEM_USE_GRAPHS=1): with
+        # several states in flight the per-setup capture costs more than the
+        # replays save at these cycle counts
+        if use_graphs is None:
+            use_graphs = os.environ.get("SIMPFEM_USE_GRAPHS", "0") == "1"
+        o.use_graphs = 1 if use_graphs else 0
         self._opts = o
         h = ctypes.c_void_p()
         _lib.call("simpfem_gmg_create", mf_op.mesh.handle, ctypes.byref(o), ctypes.byref(h))

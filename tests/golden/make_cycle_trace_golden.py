@@ -57,6 +57,10 @@ def main() -> None:
             gmg.setup(fx[f"cant24/E_{tag}"])
             tr = gmg.cycle_trace(rhs).to_dict()
             out["traces"][f"{sname}/{tag}"] = {"stack": stack, "trace": tr}
+    # one level: the trace is a single coarsest visit whose solve is the fine smoother
+    _, _, _, _, gmg = _build(spec, 1, {})
+    gmg.setup(fx["cant24/E_mid"])
+    out["traces"]["single_level/mid"] = {"stack": {}, "n_levels": 1, "trace": gmg.cycle_trace(rhs).to_dict()}
     out["diagnostics"] = {}
     for sname in ("plain_cheb", "plain_jacobi", "wcycle", "level_fp32"):
         for tag in ("hi", "mid"):

@@ -94,7 +94,7 @@ def test_records_decode_to_the_oracle_trace(ref, key):
     with open(GOLDEN) as fh:
         case = json.load(fh)["traces"][key]
     op = S.Operator(24, 12, 6, ref["cant24/free"])
-    g = GMG(op, n_levels=3, **dict(dict(fine_smoother="fp64"), **case["stack"]))
+    g = GMG(op, n_levels=case.get("n_levels", 3), **dict(dict(fine_smoother="fp64"), **case["stack"]))
     g.setup(ref[f"cant24/E_{key.split('/')[1]}"])
     tr = g.cycle_trace(ref["cant24/rhs"])
     visits, summary = encode(tr, tr["root_enrichment_mode"])

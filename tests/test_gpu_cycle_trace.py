@@ -26,7 +26,7 @@ with open(GOLDEN) as _fh:
 @pytest.mark.parametrize("key", sorted(_TRACES))
 def test_device_trace_matches_reference(cuda, ref, key):
     case = _TRACES[key]
-    _, gmg, _ = _components("cant24", case["stack"])
+    _, gmg, _ = _components("cant24", case["stack"], n_levels=case.get("n_levels", 3))
     gmg.setup(cuda.as_tensor(ref[f"cant24/E_{key.split('/')[1]}"], device="cuda"))
     got = gmg.cycle_trace(cuda.as_tensor(ref["cant24/rhs"], device="cuda")).to_dict()
     rtol = 1e-6 if key.startswith("level_fp32") else 1e-9

@@ -54,9 +54,9 @@ def assert_trace_close(got: dict, want: dict, rtol: float, path: str = "") -> No
             assert a is not None and abs(float(a) - float(b)) <= rtol * (abs(float(b)) + 1.0), (where, a, b)
 
 
-def _oracle_trace(ref, stack, tag):
+def _oracle_trace(ref, stack, tag, n_levels=3):
     op = S.Operator(24, 12, 6, ref["cant24/free"])
-    g = GMG(op, n_levels=3, **dict(dict(fine_smoother="fp64"), **stack))
+    g = GMG(op, n_levels=n_levels, **dict(dict(fine_smoother="fp64"), **stack))
     g.setup(ref[f"cant24/E_{tag}"])
     return g.cycle_trace(ref["cant24/rhs"])
 
@@ -64,7 +64,7 @@ def _oracle_trace(ref, stack, tag):
 @pytest.mark.parametrize("key", sorted(_load()["traces"]))
 def test_oracle_trace_matches_reference(ref, key):
     case = _load()["traces"][key]
-    got = _oracle_trace(ref, case["stack"], key.split("/")[1])
+    got = _oracle_trace(ref, case["stack"], key.split("/")[1], case.get("n_levels", 3))
     rtol = 1e-6 if key.startswith("level_fp32") else 1e-9
     assert_trace_close(got, case["trace"], rtol, key)
 

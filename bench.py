@@ -301,6 +301,22 @@ def run_native(args):
         fp64.run(torch.as_tensor(states[s], device="cuda"))
     ms_fp64, rows_fp64, _ = timed(fp64, timed_seeds, host_io=False)
 
+    # the mixed solve's error against the FP64 solve of the same state (untimed,
+    # after the timed regions): displacement and compliance, first 8 timed states
+    w0 = mixed.workers[0]
+    F = w0.F_free_gpu
+    fp64_err = []
+    for s in timed_seeds[:8]:
+        d = torch.as_tensor(states[s], device="cuda")
+        rm = w0.run(d)
+        xm = w0.last_x.clone()
+        rf = fp64.run(d)
+        xf = fp64.last_x
+        cm, cf = float(torch.dot(F, xm)), float(torch.dot(F, xf))
+        fp64_err.append((float(torch.linalg.norm(xm - xf) / torch.linalg.norm(xf)), abs(cm - cf) / abs(cf),
+                         rm["recommended_rho_min"] == rf["recommended_rho_min"]))
+    torch.cuda.synchronize()
+
     n_states = job_states(K, world)
     value = n_states / (ms_mixed / 1e3)
     e2e_value = n_states / (ms_e2e / 1e3)
@@ -356,6 +372,13 @@ def run_native(args):
             for s, r, f in zip(timed_seeds, rows_mixed, rows_fp64)
         ],
         "all_guarded": all(r["solve_converged"] for r in rows_mixed + rows_e2e + rows_fp64),
+        "error_vs_fp64": {
+            "states": len(fp64_err),
+            "x_rel_err_max": max(e[0] for e in fp64_err),
+            "compliance_rel_err_max": max(e[1] for e in fp64_err),
+            "same_floor": all(e[2] for e in fp64_err),
+            "note": "mixed vs FP64 solve of the same state, both stopped at true relative residual <= 1e-6",
+        },
         "policy": args.policy,
         "learned_stops_at_r50": sum(1 for r in rows_mixed + rows_e2e if r.get("stopped_at_r50")),
         "e2e": {

@@ -207,22 +207,33 @@ class LearnedFloorPolicy(GuardedFloorPolicy):
         self.dims = tuple(int(d) for d in dims)
         self.min_confidence = float(min_confidence)
 
-    def run(self, density, *, binary: bool = False) -> dict:
+    # device steps of the decision (a host test replaces them)
+    def _pool(self, density):
+        """The density average-pooled to 16^3 on the device."""
+        return self.proposer.pool(density, self.dims)
+
+    def _propose(self, pooled, features) -> np.ndarray:
+        """Softmax over the rungs for one pooled density and its two probe features."""
         torch = _lib.require_cuda()
+        prob = self.proposer.forward(pooled.reshape(1, -1),
+                                     torch.tensor([features], dtype=torch.float32, device="cuda"))
+        return prob[0].cpu().numpy()
+
+    def _sync(self) -> None:
+        _lib.require_cuda().cuda.current_stream().synchronize()
+
+    def run(self, density, *, binary: bool = False) -> dict:
         rungs = [self.baseline_rho_min] + list(self.raised_rho_mins)
         high = self.thresholds["high_residual_threshold"]
-        stream = torch.cuda.current_stream()
         t0 = time.perf_counter()
-        x = self.proposer.pool(density, self.dims)
-        stream.synchronize()
+        x = self._pool(density)
+        self._sync()
         pool_time = time.perf_counter() - t0
         dec = {"prob": None, "proposed": None, "stop": None}
 
         def at_r50(history):
             r50 = history[min(self.probe_r50, len(history) - 1)]
-            f = probe_features(r50, history, self.probe_r50, high)
-            prob = self.proposer.forward(x.reshape(1, -1), torch.tensor([f], dtype=torch.float32, device="cuda"))
-            prob = prob[0].cpu().numpy()
+            prob = self._propose(x, probe_features(r50, history, self.probe_r50, high))
             k = int(np.argmax(prob))
             dec["prob"] = prob
             dec["proposed"] = k if float(prob[k]) >= self.min_confidence else 0

@@ -57,7 +57,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--stack", default="plain", choices=["plain", "canonical"])
-    ap.add_argument("--width", type=int, default=4, help="states in flight per GPU in the mixed arm")
+    ap.add_argument("--width", type=int, default=8, help="states in flight per GPU in the mixed arm")
     ap.add_argument("--policy", default="learned", choices=["learned", "plain"],
                     help="mixed arm: learned floor proposal (decides at r50) or the plain probe-and-ladder")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -264,14 +264,16 @@ size_t simpfem_oc_work_bytes(void);
  * Heaviside projection: bisection on the multiplier over [0, 1e9] (at most 100
  * steps, until the bracket is below 1e-9) of
  * rn = clip(clip(rho sqrt(-min(dc,-1e-12) / (lm max(dv,1e-12))), rho -+ move), 1e-3, 1)
- * against sum(H rn) = volfrac n, evaluated as sum_j dv_j rn_j with dv = H^T 1.
- * rho, dc, dv, rho_new: device arrays of n doubles; work: device workspace of at
- * least simpfem_oc_work_bytes() bytes.  *change_host = max |rho_new - rho|,
+ * against sum(H rn) = volfrac n, evaluated as sum_j vol_w_j rn_j with vol_w = H^T 1.
+ * dc: the design sensitivities H^T dc_phys; dv: the volume sensitivities, NULL for
+ * ones (the reference's choice without a Heaviside projection, simp_gpu.py:262-263).
+ * rho, dc, dv, vol_w, rho_new: device arrays of n doubles; work: device workspace of
+ * at least simpfem_oc_work_bytes() bytes.  *change_host = max |rho_new - rho|,
  * *lambda_host the final multiplier, *steps_host the bisection steps (each may be
  * NULL).  Synchronises the stream once per bisection step. */
-int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const double* dv, double volfrac,
-                      double move, double* rho_new, double* work, size_t work_bytes, double* change_host,
-                      double* lambda_host, int* steps_host, void* stream);
+int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const double* dv, const double* vol_w,
+                      double volfrac, double move, double* rho_new, double* work, size_t work_bytes,
+                      double* change_host, double* lambda_host, int* steps_host, void* stream);
 
 /* ---- learned floor proposer (no counterpart in the reference) ------------------
  * A small 3D CNN over the density pooled to 16^3 plus two probe features, with a

@@ -3,9 +3,9 @@ infrastructure only).
 
 * ``oc_update`` follows the reference's GPU OC step (gpu_fem/simp_gpu.py:212-294,
   ``_oc_step_cupy`` without the Heaviside projection): design sensitivities
-  H^T dc, volume sensitivities H^T 1, bisection on the multiplier over [0, 1e9]
-  for at most 100 steps until the bracket is below 1e-9, the volume of every
-  candidate evaluated as sum(H rn) with the sparse filter matrix.
+  H^T dc, volume sensitivities 1 (:262-263), bisection on the multiplier over
+  [0, 1e9] for at most 100 steps until the bracket is below 1e-9, the volume of
+  every candidate evaluated as sum(H rn) with the sparse filter matrix.
 * ``compliance_and_sensitivity`` solves K(E) u = F directly (scipy sparse LU on
   the assembled FP64 stiffness) and returns c = F.u and
   dc = -p (1 - rho_min) rho^(p-1) u_e^T KE u_e, the SIMP sensitivity the
@@ -26,7 +26,7 @@ def oc_update(rho, dc_phys, H: sp.csr_matrix, volfrac: float, move: float):
     rho = np.asarray(rho, dtype=np.float64)
     n = rho.size
     dc_design = H.T @ np.asarray(dc_phys, dtype=np.float64)
-    dv_design = H.T @ np.ones(n)
+    dv_design = np.ones(n)
     dc_s = np.minimum(dc_design, -1e-12)
     dv_s = np.maximum(dv_design, 1e-12)
     l1, l2 = 0.0, 1e9

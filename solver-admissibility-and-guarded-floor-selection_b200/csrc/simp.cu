@@ -96,18 +96,20 @@ __device__ __forceinline__ double oc_candidate(double rho, double dc, double dv,
   return fmin(fmax(r, 1e-3), 1.0);
 }
 
-// mode 0: partial sums of dv * rn(lm); mode 1: write rn(lm) and partial maxima of |rn - rho|
+// mode 0: partial sums of vw * rn(lm) (vw = H^T 1: the filtered volume sum(H rn));
+// mode 1: write rn(lm) and partial maxima of |rn - rho|.  dv == nullptr: dv = 1.
 __global__ void __launch_bounds__(kSimpThreads) oc_pass_kernel(int64_t n, const double* __restrict__ rho,
                                                                const double* __restrict__ dc,
-                                                               const double* __restrict__ dv, double lm,
+                                                               const double* __restrict__ dv,
+                                                               const double* __restrict__ vw, double lm,
                                                                double move, int mode, double* __restrict__ rn,
                                                                double* __restrict__ partials) {
   __shared__ double sh[32];
   double v = 0.0;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const double r = oc_candidate(rho[e], dc[e], dv[e], lm, move);
+    const double r = oc_candidate(rho[e], dc[e], dv ? dv[e] : 1.0, lm, move);
     if (mode == 0) {
-      v += dv[e] * r;
+      v += vw[e] * r;
     } else {
       rn[e] = r;
       v = fmax(v, fabs(r - rho[e]));
@@ -207,11 +209,11 @@ int simpfem_cone_filter(int nx, int ny, int nz, double rmin, int transpose, cons
 
 size_t simpfem_oc_work_bytes(void) { return sizeof(double) * (kSimpBlocks + 2); }
 
-int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const double* dv, double volfrac,
-                      double move, double* rho_new, double* work, size_t work_bytes, double* change_host,
-                      double* lambda_host, int* steps_host, void* stream) {
+int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const double* dv, const double* vol_w,
+                      double volfrac, double move, double* rho_new, double* work, size_t work_bytes,
+                      double* change_host, double* lambda_host, int* steps_host, void* stream) {
   SIMP_API_BEGIN
-  if (n < 1 || !rho || !dc || !dv || !rho_new || !work) throw InvalidArg{"simpfem_oc_update: null argument"};
+  if (n < 1 || !rho || !dc || !vol_w || !rho_new || !work) throw InvalidArg{"simpfem_oc_update: null argument"};
   if (work_bytes < simpfem_oc_work_bytes()) throw InvalidArg{"simpfem_oc_update: workspace too small"};
   cudaStream_t s = (cudaStream_t)stream;
   double* partials = work;
@@ -224,7 +226,7 @@ int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const doub
   // when l2 - l1 < 1e-9; the candidate of the last midpoint is the update
   for (int it = 0; it < 100; ++it) {
     lm = 0.5 * (l1 + l2);
-    oc_pass_kernel<<<nb, kSimpThreads, 0, s>>>(n, rho, dc, dv, lm, move, 0, nullptr, partials);
+    oc_pass_kernel<<<nb, kSimpThreads, 0, s>>>(n, rho, dc, dv, vol_w, lm, move, 0, nullptr, partials);
     oc_finish_kernel<<<1, 32, 0, s>>>(nb, 0, partials, out);
     SF_CUDA(sf_launched(2));
     double vol = 0.0;
@@ -235,7 +237,7 @@ int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const doub
     else l2 = lm;
     if (l2 - l1 < 1e-9) break;
   }
-  oc_pass_kernel<<<nb, kSimpThreads, 0, s>>>(n, rho, dc, dv, lm, move, 1, rho_new, partials);
+  oc_pass_kernel<<<nb, kSimpThreads, 0, s>>>(n, rho, dc, dv, vol_w, lm, move, 1, rho_new, partials);
   oc_finish_kernel<<<1, 32, 0, s>>>(nb, 1, partials, out);
   SF_CUDA(sf_launched(2));
   double ch = 0.0;

@@ -11,8 +11,9 @@ parameter controller) with the floor policy in place of the plain solve:
    and every accepted answer checked by the FP64 recomputed true residual;
 3. compliance c = F.u and dc = -p (1 - rho_min) rho_phys^(p-1) u_e^T KE u_e
    (simpfem_element_energy), as SolverV4 returns them (solver_v4.py:257-264);
-4. the OC update of _oc_step_cupy (simp_gpu.py:212-294): H^T dc, H^T 1 and the
-   multiplier bisection (simpfem_oc_update).
+4. the OC update of _oc_step_cupy (simp_gpu.py:212-294) without the projection:
+   design sensitivities H^T dc, volume sensitivities 1 (:262-263), the multiplier
+   bisection against sum(H rn) (simpfem_oc_update, volume weights H^T 1).
 
     python simp_loop.py [--dims 200 100 50] [--iters 50] [--policy learned|plain] [--out result.json]
 
@@ -59,17 +60,21 @@ class OCUpdater:
         self._work = torch.empty((nbytes + 7) // 8, dtype=torch.float64, device="cuda")
         self._nbytes = nbytes
 
-    def __call__(self, rho, dc_design, dv_design, volfrac: float, move: float):
-        """Returns (rho_new, change, multiplier, bisection steps)."""
+    def __call__(self, rho, dc_design, vol_weights, volfrac: float, move: float, dv_design=None):
+        """Returns (rho_new, change, multiplier, bisection steps).  ``vol_weights``
+        = H^T 1 (so sum(vol_weights * rn) = sum(H rn)); ``dv_design`` the volume
+        sensitivities, None for ones as the reference has them without a projection."""
         torch = _lib.require_cuda()
         r = _lib.as_cuda(rho, torch.float64)
         dc = _lib.as_cuda(dc_design, torch.float64)
-        dv = _lib.as_cuda(dv_design, torch.float64)
+        vw = _lib.as_cuda(vol_weights, torch.float64)
+        dv = _lib.as_cuda(dv_design, torch.float64) if dv_design is not None else None
         out = torch.empty_like(r)
         ch, lm, st = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
-        _lib.call("simpfem_oc_update", int(r.numel()), _lib.ptr(r), _lib.ptr(dc), _lib.ptr(dv), float(volfrac),
-                  float(move), _lib.ptr(out), _lib.ptr(self._work), self._nbytes, ctypes.byref(ch), ctypes.byref(lm),
-                  ctypes.byref(st), _lib.stream_ptr())
+        _lib.call("simpfem_oc_update", int(r.numel()), _lib.ptr(r), _lib.ptr(dc),
+                  _lib.ptr(dv) if dv is not None else None, _lib.ptr(vw), float(volfrac), float(move), _lib.ptr(out),
+                  _lib.ptr(self._work), self._nbytes, ctypes.byref(ch), ctypes.byref(lm), ctypes.byref(st),
+                  _lib.stream_ptr())
         return out, float(ch.value), float(lm.value), int(st.value)
 
 
@@ -100,7 +105,8 @@ def run_simp_guarded(dims=(200, 100, 50), *, volfrac: float = 0.3, rmin: float =
     oc = OCUpdater()
     rng = np.random.default_rng(seed)
     rho = torch.as_tensor(np.clip(volfrac + noise * rng.standard_normal(n), 1e-3, 1.0), device="cuda")
-    dv = cone_filter(torch.ones(n, dtype=torch.float64, device="cuda"), dims, rmin, transpose=True)
+    # H^T 1: weights that turn sum(rn) into the filtered volume sum(H rn)
+    vol_w = cone_filter(torch.ones(n, dtype=torch.float64, device="cuda"), dims, rmin, transpose=True)
     F = pol.F_free_gpu
     rows = []
     t_run = time.perf_counter()
@@ -116,7 +122,7 @@ def run_simp_guarded(dims=(200, 100, 50), *, volfrac: float = 0.3, rmin: float =
         ce = element_energy(pol.mf_op, x)
         dc_phys = -penal * (1.0 - rho_min) * rho_phys.clamp_min(0.0) ** (penal - 1.0) * ce
         dc = cone_filter(dc_phys, dims, rmin, transpose=True)
-        rho_new, change, lm, steps = oc(rho, dc, dv, volfrac, move)
+        rho_new, change, lm, steps = oc(rho, dc, vol_w, volfrac, move)
         stream.synchronize()
         row = {
             "iter": it, "compliance": compliance, "volume": float(rho_phys.mean()), "change": change,

@@ -3,10 +3,11 @@ against the oracle.
 
 * the cone filter H x and H^T x against the oracle's sparse filter matrix
   (to 1e-13 of the largest entry; radii 1.2, 1.5, 2.5, ragged grids);
-* the OC update against the reference's bisection restated in oracle/simp.py,
-  which evaluates every candidate's volume as sum(H rn) through the sparse
-  matrix (the kernel uses sum_j (H^T 1)_j rn_j): same step count, multiplier
-  and new densities to the final bisection bracket (1e-8);
+* the OC update against the reference's own _oc_step_cupy outputs
+  (tests/golden/oc_reference.npz) and against its bisection restated in
+  oracle/simp.py, which evaluates every candidate's volume as sum(H rn) through
+  the sparse matrix (the kernel uses sum_j (H^T 1)_j rn_j): same step count,
+  multiplier and new densities to the final bisection bracket (1e-8);
 * the first loop iteration's compliance and sensitivities against a direct
   sparse solve (1e-6 and 1e-5 relative: the solve stops at true residual 1e-6);
 * a short loop: every solve guarded, the volume held at the target by the OC
@@ -34,6 +35,26 @@ def test_cone_filter_matches_oracle(cuda, dims, rmin):
         assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max(), t
 
 
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_oc_update_matches_reference_outputs(cuda, case):
+    """The device OC update on the inputs of the reference's own _oc_step_cupy
+    runs (tests/golden/oc_reference.npz): new densities to 1e-8 (the last
+    bisection bracket), the same change."""
+    import os
+
+    from gpu_fem.simp_loop import OCUpdater, cone_filter
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "oc_reference.npz"))
+    rmin, volfrac, move = (float(v) for v in g[f"c{case}/params"])
+    dims = (24, 12, 6)
+    n = int(np.prod(dims))
+    dc = cone_filter(cuda.as_tensor(g[f"c{case}/dc_phys"], device="cuda"), dims, rmin, transpose=True)
+    vol_w = cone_filter(cuda.ones(n, dtype=cuda.float64, device="cuda"), dims, rmin, transpose=True)
+    rn, change, _, _ = OCUpdater()(cuda.as_tensor(g[f"c{case}/rho"], device="cuda"), dc, vol_w, volfrac, move)
+    np.testing.assert_allclose(rn.cpu().numpy(), g[f"c{case}/rn"], rtol=0, atol=1e-8)
+    assert change == pytest.approx(float(g[f"c{case}/change"][0]), abs=1e-8)
+
+
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_oc_update_matches_reference_bisection(cuda, seed):
     from gpu_fem.simp_loop import OCUpdater, cone_filter
@@ -46,8 +67,8 @@ def test_oc_update_matches_reference_bisection(cuda, seed):
     H = osol.density_filter(*dims, rmin)
     ref_rn, ref_change, ref_lm, ref_steps = osimp.oc_update(rho, dc_phys, H, 0.3, 0.2)
     dc = cone_filter(cuda.as_tensor(dc_phys, device="cuda"), dims, rmin, transpose=True)
-    dv = cone_filter(cuda.ones(n, dtype=cuda.float64, device="cuda"), dims, rmin, transpose=True)
-    rn, change, lm, steps = OCUpdater()(cuda.as_tensor(rho, device="cuda"), dc, dv, 0.3, 0.2)
+    vol_w = cone_filter(cuda.ones(n, dtype=cuda.float64, device="cuda"), dims, rmin, transpose=True)
+    rn, change, lm, steps = OCUpdater()(cuda.as_tensor(rho, device="cuda"), dc, vol_w, 0.3, 0.2)
     # the bracket halves every step, so the step count is fixed; the last steps
     # compare volumes within round-off of the target, where the two (equal)
     # volume formulas may round apart: the multiplier agrees to the final

@@ -96,3 +96,34 @@ def test_ops_refuse_without_gpu():
 
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.require_cuda()
+
+
+def test_abi_rejects_bad_arguments_before_touching_the_device():
+    """Entry points added for the SIMP loop and the cycle trace check their
+    arguments first: status SIMPFEM_EINVAL (1) and a message, no CUDA call."""
+    import ctypes
+
+    from gpu_fem import _lib
+
+    lib = _lib.load()
+    fake = ctypes.c_void_p(16)  # never dereferenced: every call below fails validation first
+    nv = ctypes.c_int()
+
+    def status(name, *args):
+        st = getattr(lib, name)(*args)
+        return st, (lib.simpfem_last_error() or b"").decode()
+
+    st, msg = status("simpfem_gmg_cycle_trace", None, None, 0, None, 0, ctypes.byref(nv), None, None)
+    assert st == 1 and "cycle_trace" in msg
+    st, msg = status("simpfem_gmg_cycle_trace", fake, fake, 5, None, 0, ctypes.byref(nv), fake, None)
+    assert st == 1 and "cycle_type" in msg
+    st, msg = status("simpfem_oc_update", 0, fake, fake, None, fake, 0.3, 0.2, fake, fake, 1 << 20, None, None,
+                     None, None)
+    assert st == 1 and "oc_update" in msg
+    st, msg = status("simpfem_oc_update", 8, fake, fake, None, None, 0.3, 0.2, fake, fake, 1 << 20, None, None,
+                     None, None)
+    assert st == 1 and "oc_update" in msg  # the volume weights H^T 1 are required
+    st, msg = status("simpfem_cone_filter", 4, 4, 4, 0.5, 0, fake, ctypes.c_void_p(32), None)
+    assert st == 1 and "rmin" in msg
+    st, msg = status("simpfem_cone_filter", 4, 4, 4, 1.5, 0, fake, fake, None)
+    assert st == 1 and "cone_filter" in msg

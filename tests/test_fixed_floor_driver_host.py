@@ -47,3 +47,12 @@ def test_parse_floors_and_unknown_case():
     assert parse_floors("1e-12;1e-3,1e-2") == [1e-12, 1e-3, 1e-2]
     with pytest.raises(ValueError, match="case_type"):
         density_for_case({"case_type": "other"}, 4, ".")
+
+
+def test_parser_defaults_follow_reference():
+    """run_gmg_fixed_floor_controls.py:61-66 defaults (paths are relative here)."""
+    from gpu_fem.fixed_floor_driver import build_parser
+
+    a = build_parser().parse_args([])
+    assert (a.restart, a.maxiter, a.tol) == (300, 300, 1e-6)
+    assert a.manifest.endswith("fixed_floor_control_manifest.csv") and a.density_root == "."

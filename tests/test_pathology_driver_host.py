@@ -85,3 +85,19 @@ def test_case_table_matches_reference_run():
         assert s["family"] == c["family"] and s["seed"] == str(c["seed"])
         for k in ("volfrac", "rho_min", "penal"):
             assert float(s[k]) == c[k], (s["case"], k)
+
+
+def test_parser_defaults_follow_reference():
+    """run_pathology_diagnostics.py:209-246 defaults."""
+    from gpu_fem.pathology_driver import build_parser
+
+    a = build_parser().parse_args([])
+    assert (a.preset, a.cases, a.n_levels, a.fine_smoother, a.smoother_type, a.cycle_type) == (
+        "cantilever_gpu_medium", "hardset", 4, "fp64", "chebyshev", "v")
+    assert (a.coarse_policy, a.coarse_acceptance_ratio, a.coarse_max_scale) == ("none", 1.0, 1.0)
+    assert (a.root_enrichment_mode, a.root_enrichment_weight_floor, a.root_enrichment_weight_power) == (
+        "none", 1e-6, 0.5)
+    assert (a.root_local_correction_mode, a.root_local_correction_inner_steps,
+            a.root_local_correction_inner_restart) == ("none", 10, None)
+    assert (a.inner_fgmres_steps, a.inner_fgmres_restart, a.restart, a.maxiter, a.tol, a.skip_solve) == (
+        0, None, 50, 500, 1e-6, False)

@@ -42,3 +42,19 @@ def test_every_small_reference_preset_exists_here():
     from gpu_fem import presets
 
     assert set(_REF) <= set(presets.list_presets())
+
+
+@pytest.mark.parametrize("name", ["cantilever_3d", "cantilever_gpu_medium", "cantilever_gpu_large",
+                                  "cantilever_gpu_xlarge"])
+def test_oracle_cantilever_bc_matches_reference(name):
+    """The oracle's closed-form cantilever BCs (used by the oracle-side tests)
+    against the reference's generate_bc digests."""
+    from oracle import solver as osol
+
+    ref = _REF[name]
+    free, F = osol.cantilever_bc(*ref["grid"], *ref["domain"])
+    free = np.asarray(free, dtype=np.int64)
+    nz = np.nonzero(F)[0]
+    assert free.size == ref["n_free"]
+    assert hashlib.sha256(free.tobytes()).hexdigest() == ref["free_sha256"]
+    assert hashlib.sha256(nz.astype(np.int64).tobytes() + F[nz].tobytes()).hexdigest() == ref["load_sha256"]

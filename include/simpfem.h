@@ -32,6 +32,7 @@ enum {
   SIMPFEM_ECUDA = 2,        /* CUDA runtime failure */
   SIMPFEM_ENOTSETUP = 5,    /* apply before setup (reference raises RuntimeError) */
   SIMPFEM_ENONFINITE = 6,   /* non-finite input or result */
+  SIMPFEM_ECALLBACK = 7,    /* a caller-supplied operator callback reported a failure */
   SIMPFEM_EINTERNAL = 9
 };
 
@@ -45,6 +46,10 @@ int simpfem_version(void);
 /* Number of CUDA kernels this library has launched in the process (no reference
  * counterpart: instrumentation for benchmarks). */
 int64_t simpfem_launch_count(void);
+/* Number of device allocations (cudaMalloc) this library has made in the process
+ * (no reference counterpart: instrumentation, e.g. to check that an entry point
+ * allocates nothing). */
+int64_t simpfem_device_alloc_count(void);
 
 /* Structured hex8 mesh of nelx*nely*nelz unit elements with the given free-DOF
  * list (ascending global DOF indices) and the 24x24 unit element stiffness in
@@ -87,8 +92,10 @@ int simpfem_true_residual(simpfem_mesh* m, const double* E, const double* b_free
  * pool may forbid a library's cudaMalloc/cudaFree (allocations escape its accounting,
  * cudaFree synchronises the device); simpfem_true_residual sizes work buffers in the
  * mesh handle on first use, this entry point allocates nothing.  Inputs are
- * full-layout vectors (3 * n_nodes, 0 at constrained DOFs); r_full receives
- * b - K(E) x; *out_host = ||r|| / ||b||.  The reduction scratch is one fixed array of
+ * full-layout vectors (3 * n_nodes); x_full must hold 0 at constrained DOFs (the
+ * operator reads every entry, so a nonzero one adds its coupling K_fc x_c), while
+ * entries of b_full at constrained DOFs are ignored.  r_full receives b - K(E) x
+ * on the free DOFs and 0 elsewhere; *out_host = ||r|| / ||b|| over the free DOFs.  The reduction scratch is one fixed array of
  * about 64 KB compiled into the library and resident on every GPU that loads it; the
  * mesh may have at most 8,388,608 DOFs (SIMPFEM_EINVAL beyond).  All calls on a
  * device share that array, so calls that overlap on one GPU race: serialise them.
@@ -240,6 +247,26 @@ int simpfem_fgmres_checked(simpfem_gmg* g, const double* b_free, const double* x
 int simpfem_pcg(simpfem_gmg* g, const double* b_free, const double* x0_free, double* x_free,
                 double tol, int maxiter, double* history_host, int history_cap, int* history_len,
                 int* iters, int* converged, void* stream);
+
+/* Operator callback of the generic Krylov entry points: y = Op(x) for device
+ * vectors of n doubles; the work is enqueued on `stream` (the solve's stream)
+ * and the call returns 0, or nonzero to abort the solve (SIMPFEM_ECALLBACK). */
+typedef int (*simpfem_apply_fn)(void* ctx, const double* x, double* y, void* stream);
+/* FGMRES for any operator / preconditioner pair (_cupy_fgmres with callables that
+ * are not a hierarchy's own fine operator and apply, gpu_fem/multigrid_v4.py:416-534):
+ * the Arnoldi basis, Hessenberg, Givens rotations, back-solve and history rule of
+ * simpfem_fgmres on the device, A and M applied through the callbacks (each gets
+ * ctx).  b, x0 (may be NULL = zero start) and x are device vectors of n doubles;
+ * the host reads the convergence flags once per iteration.  Work buffers are kept
+ * per host thread and device. */
+int simpfem_fgmres_op(int64_t n, simpfem_apply_fn A, simpfem_apply_fn M, void* ctx, const double* b,
+                      const double* x0, double* x, double tol, int maxiter, int restart, double* history_host,
+                      int history_cap, int* history_len, int* iters, int* converged, void* stream);
+/* PCG for any operator / preconditioner pair (_cupy_pcg, gpu_fem/solver_v2.py:551-623):
+ * the same recurrences and history as simpfem_pcg, A and M through the callbacks. */
+int simpfem_pcg_op(int64_t n, simpfem_apply_fn A, simpfem_apply_fn M, void* ctx, const double* b, const double* x0,
+                   double* x, double tol, int maxiter, double* history_host, int history_cap, int* history_len,
+                   int* iters, int* converged, void* stream);
 
 /* Coarsest-level dense factorisation: Linv <- L^{-1}, L the lower Cholesky factor
  * of the SPD row-major n x n device matrix A (A is destroyed; Linv lower with zero

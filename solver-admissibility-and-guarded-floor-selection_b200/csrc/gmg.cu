@@ -856,110 +856,32 @@ static void base_cycle(Gmg& G, const double* rhs, double* out) {
 static void fgmres(Gmg& G, KrylovWs& K, const double* b, double* x, bool x0_zero, double tol, int maxiter,
                    int restart, const PrecFn& M, const int* parent, bool host_control, double* hist_dev,
                    int hist_cap, const CheckHook* check = nullptr) {
-  const int64_t n = G.nfull();
   Mesh& m = *G.m;
-  K.ensure(n, restart);
-  KrylovDev& kd = K.kd;
-  const int ld = restart + 1;
   const int* saved_guard = G.guard;
-  {
-    DotSet ds;
-    ds.a[0] = b;
-    ds.b[0] = b;
-    ds.nd = 1;
-    dots(G, F64, n, ds, kd.sc + SC_BNORM2, parent);
-  }
-  SF_CUDA(launch_krylov_init(kd, parent, G.st));
-  if (x0_zero) SF_CUDA(launch_fill(F64, n, 0.0, x, K.dflag(F_NOTDONE), G.st));
-  const int ncycles = (maxiter + restart - 1) / std::max(restart, 1);
-  bool stopped = false;
-  for (int c = 0; c < ncycles && !stopped; ++c) {
-    if (host_control) {
-      K.sync_flags(G.st);
-      if (K.hflags()[F_DONE]) break;
-    }
-    const int* nd = K.dflag(F_NOTDONE);
-    if (c == 0 && x0_zero) {
-      SF_CUDA(launch_copy(F64, n, b, K.r.p, nd, G.st));
-    } else {
-      EpiArgs ea;
-      ea.y = K.r.p;
-      ea.b = b;
-      ea.guard = nd;
-      fine_apply(m, F64, EPI_RESID, G.E64.p, x, ea, G.st);
-    }
-    {
-      DotSet ds;
-      ds.a[0] = K.r.p;
-      ds.b[0] = K.r.p;
-      ds.nd = 1;
-      dots(G, F64, n, ds, kd.sc + SC_BETA2, nd);
-    }
-    SF_CUDA(launch_krylov_restart(kd, tol, hist_dev, hist_cap, G.st));
-    const int* cyc = K.dflag(F_CYC);
-    SF_CUDA(launch_scale_vec(n, K.r.as<double>(), kd.sc + SC_BETA, K.Vj(0), cyc, G.st));
-    const int inner = std::min(restart, maxiter - c * restart);
-    for (int j = 0; j < inner; ++j) {
-      M(K.Vj(j), K.Zj(j), cyc);
-      G.guard = saved_guard;
-      {
-        EpiArgs ea;
-        ea.y = K.w.p;
-        ea.guard = cyc;
-        fine_apply(m, F64, EPI_APPLY, G.E64.p, K.Zj(j), ea, G.st);
-      }
-      double* Hc = kd.H + (size_t)j * ld;
-      SF_CUDA(launch_mgs_first(n, K.Vj(0), K.w.as<double>(), m.rw, Hc, cyc, G.st));
-      for (int i = 0; i <= j; ++i) {
-        const bool last = (i == j);
-        SF_CUDA(launch_mgs_step(n, K.Vj(i), last ? nullptr : K.Vj(i + 1), K.w.as<double>(), Hc + i, m.rw,
-                                last ? kd.sc + SC_HSQ : Hc + i + 1, cyc, G.st));
-      }
-      SF_CUDA(launch_givens(kd, j, tol, hist_dev, hist_cap, G.st));
-      SF_CUDA(launch_scale_vec(n, K.w.as<double>(), kd.sc + SC_HNORM, K.Vj(j + 1), cyc, G.st));
-      if (host_control) {
-        K.sync_flags(G.st);
-        if (!K.hflags()[F_CYC]) break;
-        // the caller's check at a fixed iteration count (the solve is still running):
-        // it sees the residual history so far and may end the solve here; the
-        // iterate after these columns is then formed as at the end of a cycle
-        if (check && check->fn && K.hflags()[F_TOTAL] == check->iter && hist_dev) {
-          double true_rel = NAN;
-          if (check->true_residual) {
-            // the iterate after these columns, formed in the free restart-residual
-            // vector (the back-solve writes only y), and its FP64 true residual in w
-            SF_CUDA(launch_backsolve(kd, G.st));
-            SF_CUDA(launch_copy(F64, n, x, K.r.p, nullptr, G.st));
-            SF_CUDA(launch_update_x(n, K.r.as<double>(), (double* const*)K.Zptr.p, kd.y, kd.flags, G.st));
-            EpiArgs ea;
-            ea.y = K.w.p;
-            ea.b = b;
-            fine_apply(m, F64, EPI_RESID, G.E64.p, K.r.p, ea, G.st);
-            DotSet ds;
-            ds.a[0] = K.w.p;
-            ds.b[0] = K.w.p;
-            ds.nd = 1;
-            dots(G, F64, n, ds, kd.sc + 8, nullptr);
-            double sc[9];
-            SF_CUDA(cudaMemcpyAsync(sc, kd.sc, sizeof(sc), cudaMemcpyDeviceToHost, G.st));
-            SF_CUDA(cudaStreamSynchronize(G.st));
-            true_rel = sc[SC_BNORM] > 0.0 ? sqrt(sc[8]) / sc[SC_BNORM] : 0.0;
-          }
-          const int hn = std::min(K.hflags()[F_HISTN], hist_cap);
-          check->buf.resize(hn);
-          SF_CUDA(cudaMemcpyAsync(check->buf.data(), hist_dev, sizeof(double) * hn, cudaMemcpyDeviceToHost, G.st));
-          SF_CUDA(cudaStreamSynchronize(G.st));
-          if (check->fn(check->ctx, check->iter, check->buf.data(), hn, true_rel)) {
-            stopped = true;
-            check->stopped = true;
-            break;
-          }
-        }
-      }
-    }
-    SF_CUDA(launch_backsolve(kd, G.st));
-    SF_CUDA(launch_update_x(n, x, (double* const*)K.Zptr.p, kd.y, kd.flags, G.st));
-  }
+  KrylovEnv E;
+  E.n = G.nfull();
+  E.st = G.st;
+  E.rw = m.rw;
+  E.A = [&G, &m](const double* u, double* y, const int* guard) {
+    EpiArgs ea;
+    ea.y = y;
+    ea.guard = guard;
+    fine_apply(m, F64, EPI_APPLY, G.E64.p, u, ea, G.st);
+  };
+  E.R = [&G, &m](const double* u, const double* rhs, double* r, const int* guard) {
+    EpiArgs ea;
+    ea.y = r;
+    ea.b = rhs;
+    ea.guard = guard;
+    fine_apply(m, F64, EPI_RESID, G.E64.p, u, ea, G.st);
+  };
+  // the preconditioner may move the hierarchy's skip flag; the operator's
+  // launches after it take theirs explicitly
+  PrecFn Mg = [&G, &M, saved_guard](const double* in, double* out, const int* guard) {
+    M(in, out, guard);
+    G.guard = saved_guard;
+  };
+  fgmres_core(E, K, b, x, x0_zero, tol, maxiter, restart, Mg, parent, host_control, hist_dev, hist_cap, check);
   G.guard = saved_guard;
 }
 
@@ -1457,76 +1379,26 @@ void run_pcg(Gmg& G, const double* b, double* x, double tol, int maxiter, std::v
   zb.alloc(8 * n);
   pb.alloc(8 * n);
   apb.alloc(8 * n);
-  double* r = rb.as<double>();
-  double* z = zb.as<double>();
-  double* p = pb.as<double>();
-  double* Ap = apb.as<double>();
-  double* sc = m.dscal.as<double>() + 8;
-  auto rd = [&](int k) {
-    std::vector<double> h(k);
-    SF_CUDA(cudaMemcpyAsync(h.data(), sc, sizeof(double) * k, cudaMemcpyDeviceToHost, G.st));
-    SF_CUDA(cudaStreamSynchronize(G.st));
-    return h;
+  KrylovEnv E;
+  E.n = n;
+  E.st = G.st;
+  E.rw = m.rw;
+  E.A = [&G, &m](const double* u, double* y, const int* guard) {
+    EpiArgs ea;
+    ea.y = y;
+    ea.guard = guard;
+    fine_apply(m, F64, EPI_APPLY, G.E64.p, u, ea, G.st);
   };
-  {
+  E.R = [&G, &m](const double* u, const double* rhs, double* r, const int* guard) {
     EpiArgs ea;
     ea.y = r;
-    ea.b = b;
-    fine_apply(m, F64, EPI_RESID, G.E64.p, x, ea, G.st);
-  }
-  DotSet d0;
-  d0.a[0] = b; d0.b[0] = b;
-  d0.a[1] = r; d0.b[1] = r;
-  d0.nd = 2;
-  dots(G, F64, n, d0, sc, nullptr);
-  auto h0 = rd(2);
-  const double bsq = h0[0];
-  const double tol_sq = tol * tol * bsq;
-  hist->push_back(bsq > 0 ? sqrt(h0[1] / bsq) : 0.0);
-  *iters = 0;
-  *conv = 0;
-  if (h0[1] <= tol_sq) {
-    *conv = 1;
-    return;
-  }
-  apply_full(G, r, z, nullptr);
-  SF_CUDA(launch_copy(F64, n, z, p, nullptr, G.st));
-  DotSet d1;
-  d1.a[0] = r; d1.b[0] = z; d1.nd = 1;
-  dots(G, F64, n, d1, sc, nullptr);
-  double rz = rd(1)[0];
-  int it = 1;
-  for (int k = 0; k < maxiter - 1; ++k) {
-    EpiArgs ea;
-    ea.y = Ap;
-    fine_apply(m, F64, EPI_APPLY, G.E64.p, p, ea, G.st);
-    DotSet d2;
-    d2.a[0] = p; d2.b[0] = Ap; d2.nd = 1;
-    dots(G, F64, n, d2, sc, nullptr);
-    const double pAp = rd(1)[0];
-    const double alpha = rz / pAp;
-    SF_CUDA(launch_axpby(F64, n, 1.0, x, alpha, p, x, nullptr, G.st));
-    SF_CUDA(launch_axpby(F64, n, 1.0, r, -alpha, Ap, r, nullptr, G.st));
-    DotSet d3;
-    d3.a[0] = r; d3.b[0] = r; d3.nd = 1;
-    dots(G, F64, n, d3, sc, nullptr);
-    const double rsq = rd(1)[0];
-    hist->push_back(bsq > 0 ? sqrt(rsq / bsq) : 0.0);
-    if (rsq <= tol_sq) {
-      *conv = 1;
-      break;
-    }
-    apply_full(G, r, z, nullptr);
-    it += 1;
-    DotSet d4;
-    d4.a[0] = r; d4.b[0] = z; d4.nd = 1;
-    dots(G, F64, n, d4, sc, nullptr);
-    const double rzn = rd(1)[0];
-    const double beta = rzn / rz;
-    SF_CUDA(launch_axpby(F64, n, 1.0, z, beta, p, p, nullptr, G.st));
-    rz = rzn;
-  }
-  *iters = it;
+    ea.b = rhs;
+    ea.guard = guard;
+    fine_apply(m, F64, EPI_RESID, G.E64.p, u, ea, G.st);
+  };
+  PrecFn M = [&G](const double* in, double* out, const int*) { apply_full(G, in, out, nullptr); };
+  pcg_core(E, M, b, x, tol, maxiter, rb.as<double>(), zb.as<double>(), pb.as<double>(), apb.as<double>(),
+           m.dscal.as<double>() + 8, hist, iters, conv);
 }
 
 }  // namespace simpfem

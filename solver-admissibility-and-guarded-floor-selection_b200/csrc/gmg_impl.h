@@ -21,6 +21,9 @@ struct InvalidArg {
   std::string msg;
 };
 
+// Device allocations made by the library (instrumentation, simpfem_device_alloc_count).
+void sf_count_device_alloc();
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -42,6 +45,7 @@ struct DevBuf {
     if (b <= bytes && p) return p;
     release();
     SF_CUDA(cudaMalloc(&p, b));
+    sf_count_device_alloc();
     bytes = b;
     return p;
   }
@@ -262,6 +266,31 @@ struct CheckHook {
 };
 void run_outer_fgmres(Gmg& G, const double* b, double* x, bool x0_zero, double tol, int maxiter, int restart,
                       const PrecFn& M, double* hist_dev, int hist_cap, const CheckHook* check = nullptr);
+
+// The operator side of a Krylov solve (krylov.cu): A computes y = A x and R the
+// residual r = b - A x, both skipped on the device when *guard == 0 (guard may
+// be null).  Vectors have n entries; reductions use rw on stream st.
+struct KrylovEnv {
+  int64_t n = 0;
+  cudaStream_t st = nullptr;
+  RedWork rw{};
+  std::function<void(const double* x, double* y, const int* guard)> A;
+  std::function<void(const double* x, const double* b, double* r, const int* guard)> R;
+};
+// Restarted right-preconditioned FGMRES with the Arnoldi basis, Hessenberg
+// columns, Givens rotations and back-solve on the device (_cupy_fgmres,
+// gpu_fem/multigrid_v4.py:416-534).  host_control: read the device flags after
+// every Givens update and stop launching once the cycle has ended (one
+// synchronisation per iteration); otherwise the whole solve is a fixed kernel
+// sequence whose unneeded parts are skipped by device flags.
+void fgmres_core(const KrylovEnv& E, KrylovWs& K, const double* b, double* x, bool x0_zero, double tol,
+                 int maxiter, int restart, const PrecFn& M, const int* parent, bool host_control, double* hist_dev,
+                 int hist_cap, const CheckHook* check);
+// Preconditioned CG with the up-front convergence check (_cupy_pcg,
+// gpu_fem/solver_v2.py:551-623); iters counts preconditioner applications.
+// r, z, p, Ap: n-vectors of scratch; sc: 4 device doubles.
+void pcg_core(const KrylovEnv& E, const PrecFn& M, const double* b, double* x, double tol, int maxiter, double* r,
+              double* z, double* p, double* Ap, double* sc, std::vector<double>* hist, int* iters, int* conv);
 float time_smoother_step(Gmg& G, int l, int reps);
 void run_pcg(Gmg& G, const double* b, double* x, double tol, int maxiter, std::vector<double>* hist, int* iters,
              int* conv);

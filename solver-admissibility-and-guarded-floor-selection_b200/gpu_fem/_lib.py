@@ -17,7 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsimpfem.so")
 
 F64, F32, BF16 = 0, 1, 2
-_STATUS = {1: "EINVAL", 2: "ECUDA", 5: "ENOTSETUP", 6: "ENONFINITE", 9: "EINTERNAL"}
+_STATUS = {1: "EINVAL", 2: "ECUDA", 5: "ENOTSETUP", 6: "ENONFINITE", 7: "ECALLBACK", 9: "EINTERNAL"}
 
 _lock = threading.Lock()
 _lib = None
@@ -90,6 +90,7 @@ _SIGS = {
     "simpfem_last_error": (ctypes.c_char_p, []),
     "simpfem_version": (_I, []),
     "simpfem_launch_count": (_I64, []),
+    "simpfem_device_alloc_count": (_I64, []),
     "simpfem_gmg_time_smoother_step": (_I, [_P, _I, _I, _P, _P]),
     "simpfem_mesh_create": (_I, [_I, _I, _I, _P, _I64, _P, ctypes.POINTER(_P)]),
     "simpfem_mesh_destroy": (_I, [_P]),
@@ -115,6 +116,8 @@ _SIGS = {
     "simpfem_fgmres": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _P]),
     "simpfem_fgmres_checked": (_I, [_P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
     "simpfem_pcg": (_I, [_P, _P, _P, _P, _D, _I, _P, _I, _P, _P, _P, _P]),
+    "simpfem_fgmres_op": (_I, [_I64, _P, _P, _P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _P]),
+    "simpfem_pcg_op": (_I, [_I64, _P, _P, _P, _P, _P, _P, _D, _I, _P, _I, _P, _P, _P, _P]),
     "simpfem_dense_cholesky_inverse": (_I, [_I, _P, _P, _P, _P]),
     "simpfem_cone_filter": (_I, [_I, _I, _I, _D, _I, _P, _P, _P]),
     "simpfem_oc_work_bytes": (ctypes.c_size_t, []),

@@ -11,8 +11,8 @@ Cholesky -- runs in libsimpfem on the device.
 ``_cupy_fgmres`` (:416-534) dispatches to the library's device-resident FGMRES
 when the preconditioner is a ``GalerkinMatFreeGMG.apply`` and the operator is
 that hierarchy's fine operator (checked by applying both to one probe vector);
-any other operator / preconditioner pair runs the same algorithm over torch
-tensors.
+any other operator / preconditioner pair runs on the library's device Krylov
+core (``simpfem_fgmres_op``) with the two callables applied through callbacks.
 """
 
 from __future__ import annotations
@@ -25,7 +25,7 @@ from typing import Callable, Optional
 
 import numpy as np
 
-from . import _lib
+from . import _krylov, _lib
 from ._native import to_numpy
 from .solver_v2 import MatrixFreeKff, _native_gmg
 
@@ -681,78 +681,12 @@ class GalerkinMatFreeGMG:
 
 def _cupy_fgmres(A_op: Callable, b, M_op: Callable, x0=None, tol: float = 1e-6, maxiter: int = 200,
                  restart: int = 32, history=None):
-    """Flexible restarted GMRES, right preconditioning, Givens rotations."""
+    """Flexible restarted GMRES, right preconditioning, Givens rotations (multigrid_v4.py:416-534).
+
+    A hierarchy's own fine operator and ``apply`` are solved entirely in the
+    library; any other pair of callables runs on the library's device Krylov
+    core with the two operators applied through callbacks."""
     gmg = _native_gmg(A_op, M_op)
     if gmg is not None:
         return gmg._native_fgmres(b, x0, tol, maxiter, restart, history)
-    torch = _lib.require_cuda()
-    b = _lib.as_cuda(b, torch.float64)
-    x = torch.zeros_like(b) if x0 is None else _lib.as_cuda(x0, torch.float64).clone()
-    b_norm = float(torch.linalg.norm(b))
-    if b_norm <= 1e-30:
-        return x, 0, True
-    total_iters = 0
-    converged = False
-    while total_iters < maxiter:
-        r = b - A_op(x)
-        beta = float(torch.linalg.norm(r))
-        if history is not None:
-            history.append(beta / b_norm)
-        if beta / b_norm <= tol:
-            converged = True
-            break
-        V = [r / beta]
-        Z = []
-        H = np.zeros((restart + 1, restart))
-        cs = np.zeros(restart)
-        sn = np.zeros(restart)
-        g = np.zeros(restart + 1)
-        g[0] = beta
-        inner = min(restart, maxiter - total_iters)
-        j_final = 0
-        for j in range(inner):
-            z_j = M_op(V[j])
-            Z.append(z_j)
-            w = A_op(z_j)
-            for i in range(j + 1):
-                H[i, j] = float(torch.dot(V[i], w))
-                w = w - H[i, j] * V[i]
-            H[j + 1, j] = float(torch.linalg.norm(w))
-            h_norm = H[j + 1, j]
-            if h_norm > 1e-14:
-                V.append(w / h_norm)
-            for i in range(j):
-                tmp = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
-                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
-                H[i, j] = tmp
-            denom = math.sqrt(H[j, j] ** 2 + H[j + 1, j] ** 2)
-            if denom < 1e-300:
-                cs[j], sn[j] = 1.0, 0.0
-            else:
-                cs[j] = H[j, j] / denom
-                sn[j] = H[j + 1, j] / denom
-            H[j, j] = cs[j] * H[j, j] + sn[j] * H[j + 1, j]
-            H[j + 1, j] = 0.0
-            g[j + 1] = -sn[j] * g[j]
-            g[j] = cs[j] * g[j]
-            total_iters += 1
-            j_final = j + 1
-            if history is not None:
-                history.append(abs(g[j + 1]) / b_norm)
-            if abs(g[j + 1]) / b_norm <= tol:
-                converged = True
-                break
-            if h_norm <= 1e-14:
-                converged = True
-                break
-        if j_final > 0:
-            R = np.triu(H[:j_final, :j_final])
-            try:
-                y = np.linalg.solve(R, g[:j_final].copy())
-            except np.linalg.LinAlgError:
-                y = np.linalg.lstsq(R, g[:j_final].copy(), rcond=None)[0]
-            for coeff, z_j in zip(y, Z[:j_final]):
-                x = x + float(coeff) * z_j
-        if converged:
-            break
-    return x, total_iters, converged
+    return _krylov.fgmres(A_op, b, M_op, x0=x0, tol=tol, maxiter=maxiter, restart=restart, history=history)

@@ -5,8 +5,9 @@
   (``simpfem_matvec``) replaces the expand / gather / DGEMM / bincount / restrict
   passes.
 * ``NodeBlockJacobiMF`` -- :1268-1451 (``update`` / ``apply``).
-* ``_cupy_pcg`` -- :551-623, with the library's device-resident PCG when the
-  preconditioner is a ``GalerkinMatFreeGMG`` and the operator its fine operator.
+* ``_cupy_pcg`` -- :551-623: the library's device-resident PCG when the
+  preconditioner is a ``GalerkinMatFreeGMG`` and the operator its fine operator,
+  the library's PCG core with callback operators otherwise.
 * ``_coarse_free_dofs_injection`` -- :716-763.
 
 Arrays are torch CUDA tensors (numpy inputs are moved to the device).
@@ -140,43 +141,15 @@ def _native_gmg(A, M_op):
 
 
 def _cupy_pcg(A, b, M_op, x0=None, tol=1e-5, maxiter=1000, history=None):
-    """Preconditioned CG with the up-front convergence check (solver_v2.py:551-623)."""
-    torch = _lib.require_cuda()
+    """Preconditioned CG with the up-front convergence check (solver_v2.py:551-623).
+
+    A hierarchy's own fine operator and ``apply`` run the library's PCG; any other
+    operator (a callable or a matrix) and preconditioner run on the library's
+    device PCG core with the two applied through callbacks."""
     _Aop = A if callable(A) else (lambda v, _A=A: _A @ v)
     gmg = _native_gmg(_Aop, M_op)
     if gmg is not None:
         return gmg._native_pcg(b, x0, tol, maxiter, history)
-    b = _lib.as_cuda(b, torch.float64)
-    x = _lib.as_cuda(x0, torch.float64).clone() if x0 is not None else torch.zeros_like(b)
-    r = b - _Aop(x)
-    b_norm_sq = float(torch.dot(b, b))
-    tol_sq = tol**2 * b_norm_sq
-    r_sq0 = float(torch.dot(r, r))
-    if history is not None:
-        history.append((r_sq0 / b_norm_sq) ** 0.5 if b_norm_sq > 0 else 0.0)
-    if r_sq0 <= tol_sq:
-        return x, 0, True
-    z = M_op(r)
-    p = z.clone()
-    rz = float(torch.dot(r, z))
-    converged = False
-    iters = 1
-    for _ in range(maxiter - 1):
-        Ap = _Aop(p)
-        pAp = float(torch.dot(p, Ap))
-        alpha = rz / pAp
-        x = x + alpha * p
-        r = r - alpha * Ap
-        r_sq = float(torch.dot(r, r))
-        if history is not None:
-            history.append((r_sq / b_norm_sq) ** 0.5 if b_norm_sq > 0 else 0.0)
-        if r_sq <= tol_sq:
-            converged = True
-            break
-        z = M_op(r)
-        iters += 1
-        rz_new = float(torch.dot(r, z))
-        beta = rz_new / rz
-        p = z + beta * p
-        rz = rz_new
-    return x, iters, converged
+    from . import _krylov
+
+    return _krylov.pcg(_Aop, b, M_op, x0=x0, tol=tol, maxiter=maxiter, history=history)

@@ -1,44 +1,57 @@
 """The guarded floor policy inside the SIMP loop (GuardedAdaptiveFloorSolverV4).
 
-Follows experiments/phase5/run_simp_floor_trajectory.py: ``_history_at``
-(:42-46), ``_classify_probe`` (:49-63) and ``GuardedAdaptiveFloorSolverV4``
-(:66-224), a SolverV4 whose ``solve`` runs, per SIMP iteration:
+Behaviour of experiments/phase5/run_simp_floor_trajectory.py:42-224 (the class
+the trajectory driver builds around SolverV4), built here on the decision core
+of ``gpu_fem.policy``: each ``solve`` call is a sequence of trial solves at
+fixed floors, and the first one whose recomputed FP64 residual
+||F - K u|| / ||F|| meets ``cg_tol`` is the answer.
 
-1. a probe at the base floor capped at ``guarded_probe_iters`` outer
-   iterations; if its recomputed FP64 residual already meets ``cg_tol`` it is
-   accepted ("probe_converged_keep");
-2. otherwise the r50 / r100 rule on the probe history; "keep" runs the full
-   solve at the base floor and accepts it if the guard passes (else the trigger
-   gets "_guard_failed" and the ladder follows);
-3. the ladder floors in order, accepting the first guarded solve;
-4. ``RuntimeError`` when the ladder is exhausted.
+* The probe runs at the base floor with the probe's iteration cap.  If it
+  already passes the guard it is the answer ("probe_converged_keep").
+* Otherwise the r50 / r100 rule (``policy._classify``) reads the probe history
+  and gives the plan: "keep" plans a full solve at the base floor followed by
+  the ladder (a failed full solve appends "_guard_failed" to the trigger and
+  sets the fallback flag); a raise plans the ladder alone.
+* A plan that ends without an accepted trial raises ``RuntimeError``.
 
-Every accepted answer passes ||F - K u|| / ||F|| <= cg_tol recomputed in FP64.
-Each SIMP iteration appends one row to ``policy_events``.
+Each call appends one event row (the reference's keys) to ``policy_events``.
 """
 
 from __future__ import annotations
 
+import contextlib
 import time
+from dataclasses import dataclass, field
 
+import numpy as np
+
+from .policy import _classify
 from .solver_v4 import SolverV4
 
 
-def _history_at(history, iteration: int) -> float:
-    if not history:
-        return float("inf")
-    index = min(max(iteration, 0), len(history) - 1)
-    return float(history[index])
+@dataclass
+class TrialSolve:
+    """One SolverV4 solve at a fixed floor and outer-iteration cap."""
 
+    phase: str
+    rho_min: float
+    maxiter: int
+    compliance: float
+    dc_phys: np.ndarray
+    iters: int
+    true_rel_residual: float
+    wall_time_s: float
+    history: list = field(default_factory=list)
 
-def _classify_probe(r50: float, r100: float, *, high_residual_threshold: float, plateau_residual_threshold: float,
-                    plateau_ratio_threshold: float) -> tuple[bool, str]:
-    if r50 >= high_residual_threshold:
-        return True, "high_r50"
-    ratio = r100 / max(r50, 1e-300)
-    if r100 >= plateau_residual_threshold and ratio >= plateau_ratio_threshold:
-        return True, "plateau"
-    return False, "keep"
+    def residual_at(self, iteration: int) -> float:
+        """Relative-residual history entry after ``iteration`` iterations (the last
+        entry when the solve stopped earlier; +inf without a history)."""
+        if not self.history:
+            return float("inf")
+        return float(self.history[int(np.clip(iteration, 0, len(self.history) - 1))])
+
+    def passes(self, tol: float) -> bool:
+        return self.true_rel_residual <= tol
 
 
 class GuardedAdaptiveFloorSolverV4(SolverV4):
@@ -63,74 +76,72 @@ class GuardedAdaptiveFloorSolverV4(SolverV4):
         self.last_policy_probe_r100 = float("nan")
         self.last_policy_probe_true_rel_residual = float("nan")
 
-    def _solve_with_floor(self, rho_phys, penal: float, *, rho_min: float, maxiter: int, phase: str):
-        old_emin, old_maxiter = self.Emin, self.cg_maxiter
+    # ------------------------------------------------------------ trial solves
+    @contextlib.contextmanager
+    def _at_floor(self, rho_min: float, maxiter: int):
+        saved = (self.Emin, self.cg_maxiter)
         self.Emin, self.cg_maxiter = float(rho_min), int(maxiter)
         try:
-            start = time.perf_counter()
-            compliance, dc_phys = SolverV4.solve(self, rho_phys, penal)
-            elapsed = time.perf_counter() - start
-            metrics = {"phase": phase, "rho_min": float(rho_min), "maxiter": int(maxiter),
-                       "compliance": float(compliance), "iters": int(self.last_cg_iters),
-                       "true_rel_residual": float(self.last_true_rel_residual),
-                       "history": list(self.last_cg_history), "wall_time_s": elapsed}
-            return compliance, dc_phys, metrics
+            yield
         finally:
-            self.Emin, self.cg_maxiter = old_emin, old_maxiter
+            self.Emin, self.cg_maxiter = saved
 
+    def _trial(self, rho_phys, penal: float, phase: str, rho_min: float, maxiter: int) -> TrialSolve:
+        with self._at_floor(rho_min, maxiter):
+            t0 = time.perf_counter()
+            compliance, dc_phys = SolverV4.solve(self, rho_phys, penal)
+            wall = time.perf_counter() - t0
+            return TrialSolve(phase, float(rho_min), int(maxiter), float(compliance), dc_phys,
+                              int(self.last_cg_iters), float(self.last_true_rel_residual), wall,
+                              list(self.last_cg_history))
+
+    def _plan(self, raise_floor: bool) -> list:
+        """(phase, floor) of the solves after a probe that missed the guard."""
+        keep = [] if raise_floor else [("guarded_keep_full", self.guarded_base_rho_min)]
+        return keep + [("ladder", floor) for floor in self.guarded_ladder]
+
+    # ------------------------------------------------------------------ policy
     def solve(self, rho_phys, penal: float):
-        attempted: list = []
-        compliance, dc_phys, probe = self._solve_with_floor(rho_phys, penal, rho_min=self.guarded_base_rho_min,
-                                                            maxiter=self.guarded_probe_iters, phase="probe")
-        attempted.append(probe)
-        r50 = _history_at(probe["history"], self.guarded_probe_r50)
-        r100 = _history_at(probe["history"], self.guarded_probe_iters)
-        self.last_policy_probe_r50 = r50
-        self.last_policy_probe_r100 = r100
-        self.last_policy_probe_true_rel_residual = float(probe["true_rel_residual"])
-        if probe["true_rel_residual"] <= self.cg_tol:
-            selected, trigger, fallback_used = probe, "probe_converged_keep", 0
+        probe = self._trial(rho_phys, penal, "probe", self.guarded_base_rho_min, self.guarded_probe_iters)
+        r50 = probe.residual_at(self.guarded_probe_r50)
+        r100 = probe.residual_at(self.guarded_probe_iters)
+        self.last_policy_probe_r50, self.last_policy_probe_r100 = r50, r100
+        self.last_policy_probe_true_rel_residual = probe.true_rel_residual
+        trials = [probe]
+        fallback = 0
+        if probe.passes(self.cg_tol):
+            trigger, chosen = "probe_converged_keep", probe
         else:
-            predicted_raise, trigger = _classify_probe(
+            raise_floor, trigger = _classify(
                 r50, r100, high_residual_threshold=self.guarded_high_residual_threshold,
                 plateau_residual_threshold=self.guarded_plateau_residual_threshold,
                 plateau_ratio_threshold=self.guarded_plateau_ratio_threshold)
-            selected, fallback_used = None, 0
-            if not predicted_raise:
-                compliance, dc_phys, full = self._solve_with_floor(rho_phys, penal, rho_min=self.guarded_base_rho_min,
-                                                                   maxiter=self.cg_maxiter, phase="guarded_keep_full")
-                attempted.append(full)
-                if full["true_rel_residual"] <= self.cg_tol:
-                    selected = full
-                else:
-                    fallback_used = 1
-                    trigger = f"{trigger}_guard_failed"
-            if selected is None:
-                for floor in self.guarded_ladder:
-                    compliance, dc_phys, ladder = self._solve_with_floor(rho_phys, penal, rho_min=floor,
-                                                                         maxiter=self.cg_maxiter, phase="ladder")
-                    attempted.append(ladder)
-                    if ladder["true_rel_residual"] <= self.cg_tol:
-                        selected = ladder
-                        break
-            if selected is None:
-                self.policy_events.append({
-                    "trigger": trigger, "selected_rho_min": float("nan"), "fallback_used": 1,
-                    "attempted_rho_mins": ";".join(f"{row['rho_min']:.0e}" for row in attempted),
-                    "probe_r50": r50, "probe_r100": r100, "accepted_true_rel_residual": float("nan")})
-                raise RuntimeError("guarded adaptive floor policy exhausted the ladder")
-        self.last_selected_rho_min = float(selected["rho_min"])
-        self.last_true_rel_residual = float(selected["true_rel_residual"])
-        self.last_cg_iters = int(selected["iters"])
-        self.last_cg_history = list(selected["history"])
+            chosen = None
+            for phase, floor in self._plan(raise_floor):
+                trial = self._trial(rho_phys, penal, phase, floor, self.cg_maxiter)
+                trials.append(trial)
+                if trial.passes(self.cg_tol):
+                    chosen = trial
+                    break
+                if phase == "guarded_keep_full":
+                    fallback, trigger = 1, trigger + "_guard_failed"
+        attempted = ";".join(f"{t.rho_min:.0e}" for t in trials)
+        event = {"trigger": trigger, "probe_r50": r50, "probe_r100": r100}
+        if chosen is None:
+            event.update(selected_rho_min=float("nan"), fallback_used=1, attempted_rho_mins=attempted,
+                         accepted_true_rel_residual=float("nan"))
+            self.policy_events.append(event)
+            raise RuntimeError("guarded adaptive floor policy exhausted the ladder")
+        self.last_selected_rho_min = chosen.rho_min
+        self.last_true_rel_residual = chosen.true_rel_residual
+        self.last_cg_iters = chosen.iters
+        self.last_cg_history = list(chosen.history)
         self.last_policy_trigger = trigger
-        self.last_policy_fallback_used = int(fallback_used)
-        self.last_policy_attempted_rho_mins = ";".join(f"{row['rho_min']:.0e}" for row in attempted)
-        self.policy_events.append({
-            "trigger": trigger, "selected_rho_min": self.last_selected_rho_min,
-            "fallback_used": self.last_policy_fallback_used,
-            "attempted_rho_mins": self.last_policy_attempted_rho_mins, "probe_r50": r50, "probe_r100": r100,
-            "probe_true_rel_residual": self.last_policy_probe_true_rel_residual,
-            "accepted_true_rel_residual": self.last_true_rel_residual, "accepted_iters": self.last_cg_iters,
-            "attempt_count": len(attempted), "policy_time_s": sum(float(row["wall_time_s"]) for row in attempted)})
-        return compliance, dc_phys
+        self.last_policy_fallback_used = fallback
+        self.last_policy_attempted_rho_mins = attempted
+        event.update(selected_rho_min=chosen.rho_min, fallback_used=fallback, attempted_rho_mins=attempted,
+                     probe_true_rel_residual=probe.true_rel_residual,
+                     accepted_true_rel_residual=chosen.true_rel_residual, accepted_iters=chosen.iters,
+                     attempt_count=len(trials), policy_time_s=sum(t.wall_time_s for t in trials))
+        self.policy_events.append(event)
+        return chosen.compliance, chosen.dc_phys

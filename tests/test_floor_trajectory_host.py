@@ -85,12 +85,14 @@ def test_policy_branches(monkeypatch, case):
 
 
 def test_history_and_classify():
-    assert ft._history_at([], 5) == float("inf")
-    assert ft._history_at([1.0, 0.5, 0.25], 50) == 0.25
+    t = ft.TrialSolve("probe", 1e-12, 30, 1.0, np.zeros(1), 2, 1e-3, 0.0, [])
+    assert t.residual_at(5) == float("inf")
+    t.history = [1.0, 0.5, 0.25]
+    assert t.residual_at(50) == 0.25 and t.residual_at(1) == 0.5 and t.residual_at(-3) == 1.0
     thr = dict(high_residual_threshold=1e-2, plateau_residual_threshold=1e-4, plateau_ratio_threshold=0.6)
-    assert ft._classify_probe(2e-2, 1e-3, **thr) == (True, "high_r50")
-    assert ft._classify_probe(1e-3, 7e-4, **thr) == (True, "plateau")
-    assert ft._classify_probe(1e-3, 1e-5, **thr) == (False, "keep")
+    assert ft._classify(2e-2, 1e-3, **thr) == (True, "high_r50")
+    assert ft._classify(1e-3, 7e-4, **thr) == (True, "plateau")
+    assert ft._classify(1e-3, 1e-5, **thr) == (False, "keep")
 
 
 def test_solver_v4_refuses_other_paths():

@@ -7,6 +7,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -17,7 +19,9 @@ using namespace simpfem;
 
 #include <atomic>
 static std::atomic<int64_t> g_launches{0};
+static std::atomic<int64_t> g_device_allocs{0};
 namespace simpfem {
+void sf_count_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
 cudaError_t sf_launched(int k) {
   g_launches.fetch_add(k, std::memory_order_relaxed);
   return cudaGetLastError();
@@ -56,12 +60,48 @@ struct simpfem_gmg {
 
 static cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
+// The element stiffness lives in the constant bank of each device (the sweep
+// kernels read its Walsh blocks from there), so all meshes alive on a device
+// share one.  A mesh whose stiffness differs from that of the meshes alive on
+// its device is refused; once none is left, the next mesh installs its own.
+namespace {
+struct ResidentKE {
+  double ke[576];
+  int live = 0;
+  bool installed = false;
+};
+std::mutex g_ke_mutex;
+std::map<int, ResidentKE> g_ke;
+}  // namespace
+
+static void acquire_element_constants(int device, const double* ke, const WhtBlocks& wb) {
+  std::lock_guard<std::mutex> lk(g_ke_mutex);
+  ResidentKE& r = g_ke[device];
+  const bool same = r.installed && std::memcmp(r.ke, ke, sizeof(r.ke)) == 0;
+  if (!same && r.live > 0)
+    throw InvalidArg{"simpfem_mesh_create: the element stiffness differs from the one of the " +
+                     std::to_string(r.live) + " mesh(es) alive on this device; destroy them first"};
+  if (!same) {
+    set_fine_constants(ke, wb);
+    std::memcpy(r.ke, ke, sizeof(r.ke));
+    r.installed = true;
+  }
+  r.live += 1;
+}
+
+static void release_element_constants(int device) {
+  std::lock_guard<std::mutex> lk(g_ke_mutex);
+  auto it = g_ke.find(device);
+  if (it != g_ke.end() && it->second.live > 0) it->second.live -= 1;
+}
+
 extern "C" {
 
 const char* simpfem_last_error(void) { return last_error(); }
 int simpfem_version(void) { return 10000; }
 
 int64_t simpfem_launch_count(void) { return sf_launch_count(); }
+int64_t simpfem_device_alloc_count(void) { return g_device_allocs.load(); }
 
 int simpfem_gmg_time_smoother_step(simpfem_gmg* g, int level, int reps, float* avg_ms, void* stream) {
   SF_API_BEGIN
@@ -103,7 +143,12 @@ int simpfem_mesh_create(int nelx, int nely, int nelz, const int32_t* free_dofs_h
   }
   m.Q = make_level1_Q(m.ke);
   SF_CUDA(cudaGetDevice(&m.device));
-  set_fine_constants(m.ke, m.wb);
+  try {
+    acquire_element_constants(m.device, m.ke, m.wb);
+  } catch (...) {
+    delete h;
+    throw;
+  }
   m.free_idx.alloc(4 * std::max<int64_t>(1, n_free));
   if (n_free > 0) SF_CUDA(cudaMemcpy(m.free_idx.p, m.free_h.data(), 4 * n_free, cudaMemcpyHostToDevice));
   m.mask.alloc(m.g.ndof);
@@ -117,6 +162,7 @@ int simpfem_mesh_create(int nelx, int nely, int nelz, const int32_t* free_dofs_h
 
 int simpfem_mesh_destroy(simpfem_mesh* m) {
   SF_API_BEGIN
+  if (m) release_element_constants(m->impl.device);
   delete m;
   SF_API_END
 }

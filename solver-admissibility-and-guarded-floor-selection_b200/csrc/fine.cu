@@ -54,15 +54,15 @@ void set_fine_constants(const double* ke576, const WhtBlocks& wb) {
   float w32[8][9];
   for (int b = 0; b < 8; ++b)
     for (int i = 0; i < 9; ++i) w32[b][i] = (float)wb.b[b][i];
-  cudaMemcpyToSymbol(c_wht64, wb.b, sizeof(wb.b));
-  cudaMemcpyToSymbol(c_wht32, w32, sizeof(w32));
+  SF_CUDA(cudaMemcpyToSymbol(c_wht64, wb.b, sizeof(wb.b)));
+  SF_CUDA(cudaMemcpyToSymbol(c_wht32, w32, sizeof(w32)));
   float2 w32x2[8][9];
   for (int b = 0; b < 8; ++b)
     for (int i = 0; i < 9; ++i) w32x2[b][i] = make_float2(w32[b][i], w32[b][i]);
-  cudaMemcpyToSymbol(c_wht32x2, w32x2, sizeof(w32x2));
-  cudaMemcpyToSymbol(c_keb16, keb, sizeof(keb));
-  cudaMemcpyToSymbol(c_kediag, kd, sizeof(kd));
-  cudaMemcpyToSymbol(c_kenb, nb, sizeof(nb));
+  SF_CUDA(cudaMemcpyToSymbol(c_wht32x2, w32x2, sizeof(w32x2)));
+  SF_CUDA(cudaMemcpyToSymbol(c_keb16, keb, sizeof(keb)));
+  SF_CUDA(cudaMemcpyToSymbol(c_kediag, kd, sizeof(kd)));
+  SF_CUDA(cudaMemcpyToSymbol(c_kenb, nb, sizeof(nb)));
 }
 
 template <typename T>

@@ -53,10 +53,14 @@ __device__ __forceinline__ double na_warp_sum(double v) {
   return v;
 }
 
-// |r|^2 and |b|^2 with one partial per block and the last block summing the
-// partials in block order (bitwise reproducible).
+// |r|^2 and |b|^2 over the free DOFs (mask[i] != 0), with one partial per block
+// and the last block summing the partials in block order (bitwise
+// reproducible).  The residual is already zero at constrained DOFs; b is
+// masked here so loads a caller leaves at constrained DOFs do not count, as in
+// simpfem_true_residual, which compresses b to its free entries.
 __global__ void __launch_bounds__(kNaThreads) na_norms_kernel(int64_t n, const double* __restrict__ r,
                                                               const double* __restrict__ b,
+                                                              const uint8_t* __restrict__ mask,
                                                               unsigned char* scratch) {
   double* pr = reinterpret_cast<double*>(scratch);
   double* pb = pr + kNaMaxBlocks;
@@ -71,7 +75,7 @@ __global__ void __launch_bounds__(kNaThreads) na_norms_kernel(int64_t n, const d
     const int64_t i = base + (int64_t)k * kNaThreads + threadIdx.x;
     if (i < n) {
       a += r[i] * r[i];
-      c += b[i] * b[i];
+      if (mask[i]) c += b[i] * b[i];
     }
   }
   a = na_warp_sum(a);
@@ -158,7 +162,7 @@ extern "C" int simpfem_true_residual_noalloc(simpfem_mesh* mh, const double* E, 
     ea.b = b_full;
     fine_apply(m, F64, EPI_RESID, E, x_full, ea, s);
     const int blocks = (int)((n + kNaPerBlock - 1) / kNaPerBlock);
-    na_norms_kernel<<<blocks, kNaThreads, 0, s>>>(n, r_full, b_full, scratch);
+    na_norms_kernel<<<blocks, kNaThreads, 0, s>>>(n, r_full, b_full, m.mask.as<uint8_t>(), scratch);
     SF_CUDA(sf_launched(1));
     double h[2];
     SF_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, s));

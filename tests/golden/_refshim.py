@@ -21,7 +21,12 @@ import numpy as np
 import scipy.linalg
 import scipy.sparse
 
-REF_ROOT = os.environ.get("SIMPFEM_REFERENCE_ROOT", "/root/reference")
+def _ref_root() -> str:
+    root = os.environ.get("SIMPFEM_REFERENCE_ROOT")
+    if not root or not os.path.isdir(os.path.join(root, "src", "gpu_fem")):
+        raise RuntimeError("set SIMPFEM_REFERENCE_ROOT to a checkout of the reference project "
+                           "(the folder holding src/gpu_fem and experiments/)")
+    return root
 
 
 class _Pool:
@@ -102,7 +107,7 @@ def install() -> None:
     # The shipped package __init__ pulls in modules that fail at import time;
     # register an empty package object whose __path__ points at the sources.
     pkg = types.ModuleType("gpu_fem")
-    pkg.__path__ = [os.path.join(REF_ROOT, "src", "gpu_fem")]
+    pkg.__path__ = [os.path.join(_ref_root(), "src", "gpu_fem")]
     pkg._refshim = True
     sys.modules["gpu_fem"] = pkg
     paths = importlib.import_module("gpu_fem.paths")
@@ -114,11 +119,22 @@ def load(name: str):
     return importlib.import_module(f"gpu_fem.{name}")
 
 
-COPY_ROOT = os.environ.get("SIMPFEM_REFERENCE_COPY", "/tmp/simpfem_refcopy")
+_COPY_ROOT = None
+
+
+def _copy_root() -> str:
+    """Scratch folder for copies of the reference's scripts: SIMPFEM_REFERENCE_COPY,
+    else a fresh temporary folder per process."""
+    global _COPY_ROOT
+    if _COPY_ROOT is None:
+        import tempfile
+
+        _COPY_ROOT = os.environ.get("SIMPFEM_REFERENCE_COPY") or tempfile.mkdtemp(prefix="simpfem_refcopy_")
+    return _COPY_ROOT
 
 
 def _copied_script(rel: str) -> str:
-    """Copy one reference script under COPY_ROOT and return the copy's path.
+    """Copy one reference script under the scratch folder and return the copy's path.
 
     The experiment scripts derive their root folder from their own location
     and create scratch folders beneath it at import time; running a copy keeps
@@ -126,8 +142,8 @@ def _copied_script(rel: str) -> str:
     """
     import shutil
 
-    src = os.path.join(REF_ROOT, rel)
-    dst = os.path.join(COPY_ROOT, rel)
+    src = os.path.join(_ref_root(), rel)
+    dst = os.path.join(_copy_root(), rel)
     os.makedirs(os.path.dirname(dst), exist_ok=True)
     shutil.copyfile(src, dst)
     return dst
@@ -137,6 +153,17 @@ def load_paper4_runner():
     install()
     path = _copied_script(os.path.join("experiments", "paper4", "run_experiments_e1_e10.py"))
     spec = importlib.util.spec_from_file_location("paper4_runner", path)
+    module = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(module)
+    return module
+
+
+def load_driver_module(rel: str):
+    """Import a reference experiment driver (from a copy) without running its main()."""
+    install()
+    path = _copied_script(rel)
+    _copied_script(os.path.join("experiments", "paper4", "run_experiments_e1_e10.py"))
+    spec = importlib.util.spec_from_file_location("ref_driver_" + os.path.basename(rel)[:-3], path)
     module = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(module)
     return module

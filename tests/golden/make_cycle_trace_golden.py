@@ -1,7 +1,7 @@
 """Golden traces of one multigrid cycle from the reference's own ``cycle_trace``.
 
 Run from the repository root where the reference source tree is readable
-(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_cycle_trace_golden.py
 

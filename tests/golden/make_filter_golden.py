@@ -1,7 +1,7 @@
 """Golden cone density filters from the reference's own ``_build_density_filter``.
 
 Run from the repository root where the reference source tree is readable
-(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_filter_golden.py
 

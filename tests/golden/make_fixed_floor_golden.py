@@ -1,7 +1,7 @@
 """Golden output of the reference's fixed-floor control driver.
 
 Run from the repository root where the reference source tree is readable
-(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_fixed_floor_golden.py
 
@@ -45,7 +45,7 @@ def main() -> None:
         w.writeheader()
         w.writerows(MANIFEST)
     _refshim.install()
-    dst = os.path.join(_refshim.COPY_ROOT, "fields", "gray")
+    dst = os.path.join(_refshim._copy_root(), "fields", "gray")
     os.makedirs(dst, exist_ok=True)
     np.save(os.path.join(dst, "rho.npy"), np.load(os.path.join(HERE, "density_driver_fields.npz"))["gray"])
     out = tempfile.mkdtemp(prefix="fixed_floor_")

@@ -1,7 +1,7 @@
 """Golden data for the in-loop guarded floor policy (GuardedAdaptiveFloorSolverV4).
 
 Run from the repository root where the reference source tree is readable
-(default /root/reference; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_floor_trajectory_golden.py
 

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
 Run from the repository root on a machine where the reference source tree is
-readable (default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+readable (its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_golden.py
 
@@ -240,7 +240,7 @@ def make_policy(tmpdir):
 
 
 def extract_published():
-    root = os.path.join(_refshim.REF_ROOT, "data", "analysis_tables")
+    root = os.path.join(_refshim._ref_root(), "data", "analysis_tables")
     keep = {
         "gmg_fixed_floor_controls_strict_true_residual__fixed_floor_control_comparison.csv":
             "published_fixed_floor_controls.csv",
@@ -263,7 +263,7 @@ def extract_published():
         w.writeheader()
         for r in rows:
             w.writerow({c: r[c] for c in cols})
-    dens = os.path.join(_refshim.REF_ROOT, "data", "optimized_density_inputs")
+    dens = os.path.join(_refshim._ref_root(), "data", "optimized_density_inputs")
     for case in ("C64_MF", "C512_MF"):
         rho = np.load(os.path.join(dens, f"{case}__rho_final.npy"))
         np.savez_compressed(os.path.join(HERE, f"density_{case}.npz"), rho=rho)
@@ -275,7 +275,7 @@ def main():
     for name, (spec, n_levels) in _cases().items():
         make_case(name, spec, n_levels, out)
     np.savez_compressed(os.path.join(HERE, "reference_small.npz"), **out)
-    tmp = os.path.join(_refshim.COPY_ROOT, "policy_out")
+    tmp = os.path.join(_refshim._copy_root(), "policy_out")
     os.makedirs(tmp, exist_ok=True)
     make_policy(tmp)
     extract_published()

@@ -1,7 +1,7 @@
 """Golden OC updates from the reference's own ``_oc_step_cupy``.
 
 Run from the repository root where the reference source tree is readable
-(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_oc_golden.py
 

@@ -1,7 +1,7 @@
 """Golden output of the reference's pathology diagnostics driver.
 
 Run from the repository root where the reference source tree is readable
-(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_pathology_golden.py
 

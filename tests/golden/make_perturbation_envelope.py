@@ -1,7 +1,7 @@
 """Iteration-count envelope of the reference's own fixed-floor controls under round-off.
 
 Run from the repository root where the reference source tree is readable
-(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_perturbation_envelope.py [pert_seed ...]
 

@@ -1,7 +1,7 @@
 """Golden boundary conditions of the reference presets.
 
 Run from the repository root where the reference source tree is readable
-(default ``/root/reference``; override with SIMPFEM_REFERENCE_ROOT):
+(its root given by SIMPFEM_REFERENCE_ROOT):
 
     python tests/golden/make_presets_golden.py
 

@@ -16,7 +16,14 @@ one hierarchy and CUDA stream per worker), each worker a LearnedFloorPolicy
 with the committed floor proposer (``--policy plain`` for the probe-and-ladder
 alone); ``learned_stops_at_r50`` counts the states whose probe the proposal or
 the r50 rule ended early.  The ``fp64`` object is the plain FP64 form from
-scratch, one state at a time, on the same states.
+scratch, one state at a time, on the same states.  ``mixed_width1`` is the mixed
+form one state at a time (precision without concurrency); ``like_for_like``
+repeats both forms with the probe re-solved at a kept floor, as the reference
+driver does.  ``error_vs_oracle`` compares the FP64 and the mixed GPU answers of
+the first two timed states with the oracle's complete solves of the same states,
+whose time is the ``cpu_baseline``; ``--impl reference`` solves those same states.
+Two rooflines: the FP32 fused smoothing step and the FP64 operator product,
+each launch timed alone after 256 MB of pseudo-random writes evict the L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--width B] [--policy learned|plain]
                     [--impl native|reference]
@@ -62,6 +69,11 @@ def _args():
                     help="mixed arm: learned floor proposal (decides at r50) or the plain probe-and-ladder")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
+
+
+def timed_seed_start(warmup: int, width: int) -> int:
+    """Index of the first timed state: the batched arm's warm-up takes max(W, 2B) states."""
+    return max(warmup, 2 * max(1, width))
 
 
 def rank_seeds(rank: int, n: int) -> list:
@@ -218,7 +230,7 @@ def run_native(args):
     H = _filter()
     spec = cantilever_spec(NX, NY, NZ)
     K, W, B = args.steps, args.warmup, max(1, args.width)
-    WB = max(W, 2 * B)  # warm-up states for the batched arm: every worker sees at least two
+    WB = timed_seed_start(W, B)  # warm-up states for the batched arm: every worker sees at least two
     seeds = rank_seeds(rank, WB + 2 * K)
     states = {s: make_state(H, s) for s in seeds}
 
@@ -301,6 +313,19 @@ def run_native(args):
         fp64.run(torch.as_tensor(states[s], device="cuda"))
     ms_fp64, rows_fp64, _ = timed(fp64, timed_seeds, host_io=False)
 
+    # the same forms with the probe re-solved at a kept floor, as the reference
+    # driver does (like for like with the reference arm), and the mixed form one
+    # state at a time (what precision buys without concurrency)
+    for w in mixed.workers:
+        w.reuse_probe = False
+    fp64.reuse_probe = False
+    ms_mixed_nr, rows_mixed_nr, _ = timed_batch(mixed, timed_seeds, host_io=False)
+    ms_fp64_nr, rows_fp64_nr, _ = timed(fp64, timed_seeds, host_io=False)
+    for w in mixed.workers:
+        w.reuse_probe = True
+    fp64.reuse_probe = True
+    ms_mixed_w1, rows_mixed_w1, _ = timed(mixed.workers[0], timed_seeds, host_io=False)
+
     # the mixed solve's error against the FP64 solve of the same state (untimed,
     # after the timed regions): displacement and compliance, first 8 timed states
     w0 = mixed.workers[0]
@@ -329,6 +354,11 @@ def run_native(args):
               _lib.stream_ptr())
     ndof = 3 * (NX + 1) * (NY + 1) * (NZ + 1)
     ne = NX * NY * NZ
+    # the FP64 operator product of every FGMRES iteration and of the guard
+    avg64 = ctypes.c_float()
+    _lib.call("simpfem_gmg_time_operator", fp64.gmg._h, 50, ctypes.byref(avg64), _lib.stream_ptr())
+    op_bytes = 8 * ne + 2 * 8 * ndof + ndof  # read E and u, write y (FP64), 1-byte DOF mask
+    op_flops = 1152 * ne                     # 2 x 24 x 24 per element, the reference's convention
     # fp32 vectors read u, rhs, dinv (plus d for Chebyshev) and write x (plus d); E (fp32); 1-byte DOF mask
     nvec = 4 if args.stack == "plain" else 6
     alg_bytes = nvec * 4 * ndof + 4 * ne + ndof
@@ -363,6 +393,20 @@ def run_native(args):
             "unit": "guarded solves/s",
             "s_per_solve": round(ms_fp64 / K / 1e3, 5),
             "speedup_mixed_over_fp64": round(ms_fp64 / ms_mixed, 3),
+        },
+        "mixed_width1": {
+            "value": round(n_states / (ms_mixed_w1 / 1e3), 4),
+            "unit": "guarded solves/s",
+            "speedup_over_fp64": round(ms_fp64 / ms_mixed_w1, 3),
+            "note": "the mixed form one state at a time: what precision buys without concurrency",
+        },
+        "like_for_like": {
+            "mixed_value": round(n_states / (ms_mixed_nr / 1e3), 4),
+            "fp64_value": round(n_states / (ms_fp64_nr / 1e3), 4),
+            "unit": "guarded solves/s",
+            "speedup_mixed_over_fp64": round(ms_fp64_nr / ms_mixed_nr, 3),
+            "all_guarded": all(r["solve_converged"] for r in rows_mixed_nr + rows_fp64_nr),
+            "note": "probe re-solved at a kept floor (reuse_probe off), as the reference driver does",
         },
         "solves": [
             {"seed": s, "trigger": r["trigger"], "rho_min": r["recommended_rho_min"],
@@ -400,41 +444,87 @@ def run_native(args):
             "algorithmic_bytes_per_launch": alg_bytes,
             "avg_launch_us": round(avg.value * 1e3, 3),
         },
+        "roofline_fp64_operator": {
+            "kernel": "fine_sweep_kernel<double, EPI_APPLY> (FP64 operator product, cold L2)",
+            "bound": "hbm",
+            "achieved": round(op_bytes / (avg64.value * 1e-3) / 1e9, 1),
+            "peak": hbm_peak,
+            "peak_kind": peak_kind,
+            "unit": "GB/s",
+            "frac": round(op_bytes / (avg64.value * 1e-3) / 1e9 / hbm_peak, 4),
+            "traffic": _traffic_per_launch().get("fine_op_fp64"),
+            "algorithmic_bytes_per_launch": op_bytes,
+            "gflops_reference_convention": round(op_flops / (avg64.value * 1e-3) / 1e9, 1),
+            "avg_launch_us": round(avg64.value * 1e3, 3),
+        },
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(states[timed_seeds[0]], rows_fp64[0])
+        # the oracle (the reference's FP64 method on numpy/scipy) solves the first two
+        # timed states completely; its answers judge both GPU forms, and its time is
+        # the CPU baseline
+        n_or = 2
+        orc = oracle_solves([states[s] for s in timed_seeds[:n_or]])
+        errs = []
+        for k, s in enumerate(timed_seeds[:n_or]):
+            d = torch.as_tensor(states[s], device="cuda")
+            ref = orc["results"][k]
+            xo = torch.as_tensor(ref["x"], device="cuda")
+            co = float(torch.dot(F, xo))
+            for form, pol in (("fp64", fp64), ("mixed", w0)):
+                r = pol.run(d)
+                x = pol.last_x
+                errs.append({"seed": s, "form": form,
+                             "x_rel_err": float(torch.linalg.norm(x - xo) / torch.linalg.norm(xo)),
+                             "compliance_rel_err": abs(float(torch.dot(F, x)) - co) / abs(co),
+                             "same_decisions": r["recommended_rho_min"] == ref["rho_min"]
+                             and r["trigger"] == ref["trigger"] and bool(r["solve_converged"]) == ref["converged"],
+                             "true_residual": r["solve_final_rel_residual"]})
+        result["error_vs_oracle"] = {
+            "states": n_or,
+            "per_solve": errs,
+            "fp64_x_rel_err_max": max(e["x_rel_err"] for e in errs if e["form"] == "fp64"),
+            "fp64_compliance_rel_err_max": max(e["compliance_rel_err"] for e in errs if e["form"] == "fp64"),
+            "mixed_x_rel_err_max": max(e["x_rel_err"] for e in errs if e["form"] == "mixed"),
+            "mixed_compliance_rel_err_max": max(e["compliance_rel_err"] for e in errs if e["form"] == "mixed"),
+            "same_decisions": all(e["same_decisions"] for e in errs),
+            "note": "GPU answers of the first timed states against the oracle's complete FP64 guarded solves "
+                    "of the same states (all stopped at true relative residual <= 1e-6)",
+        }
+        result["cpu_baseline"] = orc["cpu_baseline"]
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
-def cpu_baseline(density, fp64_row) -> dict:
-    """The oracle (the reference's FP64 method on numpy/scipy) on a bounded sample of
-    one state: one hierarchy setup plus two outer FGMRES iterations, scaled to a
-    full guarded solve with the setup and outer-iteration counts the identical FP64
-    algorithm needed on the GPU for the same state."""
+def oracle_solves(densities) -> dict:
+    """The oracle (the reference's FP64 method on numpy/scipy: damped-Jacobi 4-level
+    GMG, FGMRES restart 300, the guarded policy with the probe re-solved at a kept
+    floor, as the reference driver does) on complete guarded solves of the given
+    512k states, in order through one hierarchy, on all host cores."""
     from oracle.gmg import GMG
-    from oracle.solver import Operator, cantilever_bc, fgmres
+    from oracle.policy import run_state
+    from oracle.solver import Operator, cantilever_bc
 
     cores = len(os.sched_getaffinity(0))
     free, F = cantilever_bc(NX, NY, NZ)
     op = Operator(NX, NY, NZ, free)
     Ff = F[free]
     g = GMG(op, n_levels=4, fine_smoother="fp64", smoother_type="jacobi")
-    E = 1e-12 + (1 - 1e-12) * density ** 3
-    t0 = time.perf_counter()
-    g.setup(E)
-    t_setup = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    fgmres(lambda v: op.matvec(v, E), Ff, g.apply, tol=1e-6, maxiter=2, restart=300)
-    t_two = time.perf_counter() - t0
-    iters, setups = int(fp64_row["total_iters"]), int(fp64_row["n_setups"])
-    t_solve = setups * t_setup + iters * (t_two / 2.0)
-    return {"value": round(1.0 / t_solve, 6), "unit": "guarded solves/s", "cores": cores, "kind": "port",
-            "sample": f"oracle setup ({t_setup:.1f} s) + 2 FGMRES iterations ({t_two:.1f} s) on one 512k state, "
-                      f"scaled to {setups} setups + {iters} iterations",
-            "s_per_solve": round(t_solve, 2)}
+    results, times = [], []
+    for d in densities:
+        t0 = time.perf_counter()
+        res = run_state(op, g, Ff, lambda rm, d=d: d, penal=3.0, raised=(1e-3, 1e-2), restart=300, maxiter=300)
+        times.append(time.perf_counter() - t0)
+        sel = res["selected"]
+        results.append({"x": sel["x"], "rho_min": sel["rho_min"], "trigger": res["trigger"],
+                        "converged": bool(sel["converged"])})
+    v = len(times) / sum(times)
+    return {"results": results, "times": times,
+            "cpu_baseline": {"value": round(v, 6), "unit": "guarded solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{len(times)} complete guarded solves of the first timed 512k states "
+                                       f"(oracle, numpy/scipy FP64; {', '.join(f'{t:.1f}' for t in times)} s)",
+                             "s_per_solve": round(sum(times) / len(times), 2)}}
 
 
 def run_reference(args):
@@ -452,9 +542,11 @@ def run_reference(args):
     Ff = F[free]
     g = GMG(op, n_levels=4, fine_smoother="fp64", smoother_type="jacobi")
     steps = max(1, min(args.steps, 2))
+    # the same states as the native arm's first timed states
+    first = timed_seed_start(args.warmup, args.width)
     times = []
     for i in range(steps):
-        d = make_state(H, args.warmup + i)
+        d = make_state(H, first + i)
         t0 = time.perf_counter()
         run_state(op, g, Ff, lambda rm, d=d: d, penal=3.0, raised=(1e-3, 1e-2), restart=300, maxiter=300)
         times.append(time.perf_counter() - t0)
@@ -467,7 +559,8 @@ def run_reference(args):
         "config": {"workload": "guarded SIMP-floor solve, cantilever 160x80x40 (512,000 elements), damped-Jacobi "
                                "4-level GMG, FGMRES restart 300 tol 1e-6, floors 1e-12|1e-3,1e-2"},
         "cpu_baseline": {"value": round(v, 6), "unit": "guarded solves/s", "cores": cores, "kind": "port",
-                         "sample": f"{steps} complete guarded solves (oracle, numpy/scipy FP64)"},
+                         "sample": f"{steps} complete guarded solves of seeds {first}..{first + steps - 1}, the "
+                                   "native arm's first timed states (oracle, numpy/scipy FP64)"},
         "e2e": {"value": round(v, 6), "unit": "guarded solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 

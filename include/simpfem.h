@@ -208,10 +208,17 @@ int simpfem_gmg_props_get(simpfem_gmg* g, simpfem_gmg_props* out);
 /* Average device time (ms) of one fused smoothing step of `level` (below the
  * coarsest) -- the operator kernel with the smoother's update fused into its
  * store, the kernel the cycle launches most -- over `reps` launches, each timed by
- * its own CUDA event pair on `stream` after a 256 MB write that evicts the L2, on
+ * its own CUDA event pair on `stream` after 256 MB of pseudo-random values are
+ * written (twice the L2, data it cannot hold compressed), on
  * pseudo-random input vectors; clobbers that level's cycle vectors (no reference
  * counterpart: instrumentation for the roofline report). */
 int simpfem_gmg_time_smoother_step(simpfem_gmg* g, int level, int reps, float* avg_ms, void* stream);
+/* Average device time (ms) of the FP64 fine operator product y = K(E) u -- the
+ * product of every outer FGMRES iteration and of the guard -- with the moduli of
+ * the last setup, timed like simpfem_gmg_time_smoother_step (cold L2, own event
+ * pair per launch); clobbers the hierarchy's FP64 scratch vectors (no reference
+ * counterpart: instrumentation for the roofline report). */
+int simpfem_gmg_time_operator(simpfem_gmg* g, int reps, float* avg_ms, void* stream);
 /* Forget the cached lambda_max estimates (the next setup re-estimates). */
 int simpfem_gmg_reset_lambda_cache(simpfem_gmg* g);
 /* Copy the fine-level operator of the last setup: E as FP64 (n_elem). */

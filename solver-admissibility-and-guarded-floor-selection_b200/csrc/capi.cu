@@ -114,6 +114,16 @@ int simpfem_gmg_time_smoother_step(simpfem_gmg* g, int level, int reps, float* a
   SF_API_END
 }
 
+int simpfem_gmg_time_operator(simpfem_gmg* g, int reps, float* avg_ms, void* stream) {
+  SF_API_BEGIN
+  if (!g || !avg_ms || reps < 1) throw InvalidArg{"simpfem_gmg_time_operator: invalid argument"};
+  Gmg& G = *g->impl;
+  if (!G.is_setup) throw NotSetup{"GalerkinMatFreeGMG.setup() must be called before apply()."};
+  G.st = S(stream);
+  *avg_ms = time_fine_operator(G, reps);
+  SF_API_END
+}
+
 int simpfem_mesh_create(int nelx, int nely, int nelz, const int32_t* free_dofs_host, int64_t n_free,
                         const double* ke_unit_host, simpfem_mesh** out) {
   SF_API_BEGIN

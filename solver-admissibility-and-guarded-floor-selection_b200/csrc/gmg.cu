@@ -1337,18 +1337,24 @@ float time_smoother_step(Gmg& G, int l, int reps) {
   const int psel = (vt == F32) ? p : F64;
   G.guard = nullptr;
   level_op(G, l, vt, psel, epi, x, ea);
-  // each rep starts from a cold L2: a 256 MB buffer (twice the L2) is written
-  // between reps, and only the step itself is inside its event pair
+  return time_cold([&]() { level_op(G, l, vt, psel, epi, x, ea); }, reps, G.st);
+}
+
+// Average device time of `launch` over `reps` runs, each from a cold L2: a
+// 256 MB buffer (twice the L2) is overwritten with pseudo-random values (data
+// the L2 cannot hold compressed) between runs, and only the launch itself is
+// inside its event pair.
+float time_cold(const std::function<void()>& launch, int reps, cudaStream_t st) {
   DevBuf flush;
-  const size_t flush_bytes = size_t(256) << 20;
-  flush.alloc(flush_bytes);
+  const int64_t flush_vals = int64_t(64) << 20;  // 64 Mi floats = 256 MB
+  flush.alloc(sizeof(float) * flush_vals);
   std::vector<cudaEvent_t> ev(2 * reps);
   for (auto& e : ev) SF_CUDA(cudaEventCreate(&e));
   for (int r = 0; r < reps; ++r) {
-    SF_CUDA(cudaMemsetAsync(flush.p, r & 0xff, flush_bytes, G.st));
-    SF_CUDA(cudaEventRecord(ev[2 * r], G.st));
-    level_op(G, l, vt, psel, epi, x, ea);
-    SF_CUDA(cudaEventRecord(ev[2 * r + 1], G.st));
+    SF_CUDA(launch_fill_hash(F32, flush_vals, 0x9e3779b9u * (uint32_t)(r + 1), flush.p, st));
+    SF_CUDA(cudaEventRecord(ev[2 * r], st));
+    launch();
+    SF_CUDA(cudaEventRecord(ev[2 * r + 1], st));
   }
   SF_CUDA(cudaEventSynchronize(ev.back()));
   float total = 0.f;
@@ -1359,6 +1365,19 @@ float time_smoother_step(Gmg& G, int l, int reps) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   return total / reps;
+}
+
+// The FP64 fine operator product y = K(E) u of the outer FGMRES (and of the
+// guard) on pseudo-random u, with the hierarchy's moduli of the last setup.
+float time_fine_operator(Gmg& G, int reps) {
+  const int64_t n = G.nfull();
+  double* u = G.tmp64a.as<double>();
+  double* y = G.tmp64b.as<double>();
+  SF_CUDA(launch_fill_hash(F64, n, 21u, u, G.st));
+  EpiArgs ea;
+  ea.y = y;
+  fine_apply(*G.m, F64, EPI_APPLY, G.E64.p, u, ea, G.st);
+  return time_cold([&]() { fine_apply(*G.m, F64, EPI_APPLY, G.E64.p, u, ea, G.st); }, reps, G.st);
 }
 
 // Outer FGMRES: host-controlled (one synchronisation per iteration to read the

@@ -292,6 +292,8 @@ void fgmres_core(const KrylovEnv& E, KrylovWs& K, const double* b, double* x, bo
 void pcg_core(const KrylovEnv& E, const PrecFn& M, const double* b, double* x, double tol, int maxiter, double* r,
               double* z, double* p, double* Ap, double* sc, std::vector<double>* hist, int* iters, int* conv);
 float time_smoother_step(Gmg& G, int l, int reps);
+float time_fine_operator(Gmg& G, int reps);
+float time_cold(const std::function<void()>& launch, int reps, cudaStream_t st);
 void run_pcg(Gmg& G, const double* b, double* x, double tol, int maxiter, std::vector<double>* hist, int* iters,
              int* conv);
 

@@ -92,6 +92,7 @@ _SIGS = {
     "simpfem_launch_count": (_I64, []),
     "simpfem_device_alloc_count": (_I64, []),
     "simpfem_gmg_time_smoother_step": (_I, [_P, _I, _I, _P, _P]),
+    "simpfem_gmg_time_operator": (_I, [_P, _I, _P, _P]),
     "simpfem_mesh_create": (_I, [_I, _I, _I, _P, _I64, _P, ctypes.POINTER(_P)]),
     "simpfem_mesh_destroy": (_I, [_P]),
     "simpfem_mesh_info": (_I, [_P, _P, _P, _P]),

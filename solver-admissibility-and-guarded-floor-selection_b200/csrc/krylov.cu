@@ -286,7 +286,11 @@ int simpfem_fgmres_op(int64_t n, simpfem_apply_fn A, simpfem_apply_fn M, void* c
   const int cap = maxiter + maxiter / std::max(restart, 1) + 4;
   OpWork& W = op_work();
   W.ensure(n, cap);
-  if (x0 && x0 != x) SF_CUDA(cudaMemcpyAsync(x, x0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  // the zero start is written here: the core skips its own fill when b is zero
+  if (x0 == nullptr)
+    SF_CUDA(launch_fill(F64, n, 0.0, x, nullptr, st));
+  else if (x0 != x)
+    SF_CUDA(cudaMemcpyAsync(x, x0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   KrylovEnv E = callback_env(W, n, A, ctx, st);
   fgmres_core(E, W.K, b, x, x0 == nullptr, tol, maxiter, restart, callback_prec(M, ctx, st), nullptr, true,
               W.hist.as<double>(), cap, nullptr);

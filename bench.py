@@ -27,6 +27,8 @@ each launch timed alone after 256 MB of pseudo-random writes evict the L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--width B] [--policy learned|plain]
                     [--impl native|reference]
+    python bench.py --kernel smoother-step|operator|dense|policy [--grid NX NY NZ] [--reps R]
+                    [--precision fp32|fp64] [--stack plain|canonical] [--dense-n N --band BW]
 
 N > 1 (torchrun): ranks solve disjoint states, no collective on the data path;
 the reported value is all states / max-over-ranks time.
@@ -68,7 +70,111 @@ def _args():
     ap.add_argument("--policy", default="learned", choices=["learned", "plain"],
                     help="mixed arm: learned floor proposal (decides at r50) or the plain probe-and-ladder")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # single-kernel launches for timing and ncu captures (no bench line)
+    ap.add_argument("--kernel", default=None, choices=["smoother-step", "operator", "dense", "policy"],
+                    help="time one library kernel (or one guarded solve) instead of the benchmark")
+    ap.add_argument("--grid", type=int, nargs=3, default=[NX, NY, NZ], metavar=("NX", "NY", "NZ"))
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--dense-n", type=int, default=3960)
+    ap.add_argument("--band", type=int, default=None)
+    ap.add_argument("--restart", type=int, default=300)
     return ap.parse_args()
+
+
+def run_kernel(args) -> None:
+    """One library kernel launched standalone: ``smoother-step`` (the fused fine
+    smoothing step, simpfem_gmg_time_smoother_step) and ``operator`` (the FP64
+    operator product, simpfem_gmg_time_operator) on the 4-level hierarchy of an
+    NX x NY x NZ cantilever with random E in [1e-3, 1.001), each launch timed alone
+    from a cold L2; ``dense`` the coarsest factorisation
+    (simpfem_dense_cholesky_inverse) of a random SPD matrix, banded with --band;
+    ``policy`` one guarded solve after three warm-up states, bracketed by
+    cudaProfilerStart/Stop for ncu --profile-from-start off.  Exits 0 on success,
+    so the same command line can run under ncu afterwards."""
+    import torch
+
+    from gpu_fem import _lib
+
+    nx, ny, nz = args.grid
+    ndof, ne = 3 * (nx + 1) * (ny + 1) * (nz + 1), nx * ny * nz
+    if args.kernel in ("smoother-step", "operator"):
+        from gpu_fem.paper4 import _build_components
+        from gpu_fem.presets import cantilever_spec
+
+        st = _stack(args.stack, "mixed" if args.precision == "fp32" else "fp64")
+        cyc = "fp32" if args.precision == "fp32" else "fp64"
+        gmg = _build_components(cantilever_spec(nx, ny, nz), cycle_precision=cyc, **st)[-1]
+        gmg.setup(torch.as_tensor(1e-3 + np.random.default_rng(0).random(ne), device="cuda"))
+        avg = ctypes.c_float()
+        if args.kernel == "smoother-step":
+            _lib.call("simpfem_gmg_time_smoother_step", gmg._h, 0, args.reps, ctypes.byref(avg), _lib.stream_ptr())
+            s = 4 if args.precision == "fp32" else 8
+            alg = (4 if args.stack == "plain" else 6) * s * ndof + s * ne + ndof
+        else:
+            _lib.call("simpfem_gmg_time_operator", gmg._h, args.reps, ctypes.byref(avg), _lib.stream_ptr())
+            alg = 8 * ne + 2 * 8 * ndof + ndof
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel": args.kernel, "grid": [nx, ny, nz], "precision": args.precision,
+                          "stack": args.stack, "avg_us": round(avg.value * 1e3, 3),
+                          "algorithmic_bytes": alg, "gbs": round(alg / (avg.value * 1e-3) / 1e9, 1)}))
+    elif args.kernel == "dense":
+        n = args.dense_n
+        g = torch.Generator(device="cuda")
+        g.manual_seed(0)
+        if args.band is None:
+            Q = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+            A0 = Q @ Q.T / n + torch.eye(n, dtype=torch.float64, device="cuda")
+        else:
+            R = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+            i = torch.arange(n, device="cuda")
+            A0 = torch.where((i[:, None] - i[None, :]).abs() <= args.band, R, torch.zeros_like(R))
+            A0 = torch.tril(A0, -1) + torch.tril(A0, -1).T + torch.diag(
+                torch.full((n,), 2.0 * args.band + 2.0, dtype=torch.float64, device="cuda"))
+        A, Li = torch.empty_like(A0), torch.empty_like(A0)
+        info = ctypes.c_int()
+        times = []
+        for _ in range(args.reps):
+            A.copy_(A0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.call("simpfem_dense_cholesky_inverse", n, _lib.ptr(A), _lib.ptr(Li), ctypes.byref(info),
+                      _lib.stream_ptr())
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        if info.value != 0:
+            raise SystemExit(f"factorisation failed: info {info.value}")
+        print(json.dumps({"kernel": "dense", "n": n, "band": args.band, "best_ms": round(min(times), 4),
+                          "median_ms": round(statistics.median(times), 4)}))
+    else:
+        from gpu_fem.policy import GuardedFloorPolicy
+        from gpu_fem.presets import cantilever_spec
+        from gpu_fem.pub_simp_solver import _build_density_filter
+
+        H = _build_density_filter(nx, ny, 1.5, nz)
+        prec = "mixed" if args.precision == "fp32" else "fp64"
+        pol = GuardedFloorPolicy(cantilever_spec(nx, ny, nz), penal=3.0, tol=1e-6, restart=args.restart,
+                                 maxiter=args.restart, probe_iters=100, probe_r50=50, raised_rho_mins=(1e-3, 1e-2),
+                                 stack=_stack(args.stack, prec), cycle_precision="fp32" if prec == "mixed" else "fp64")
+
+        def state(seed):
+            solid = (np.random.default_rng(seed).random(ne) >= 0.35).astype(np.float64)
+            return torch.as_tensor(np.asarray(H @ solid), device="cuda")
+
+        for seed in range(3):
+            pol.run(state(seed))
+        d = state(3)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        r = pol.run(d)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"kernel": "policy", "grid": [nx, ny, nz], "precision": prec,
+                          "iters": r["total_iters"], "floor": r["recommended_rho_min"],
+                          "setup_ms": round(r["probe_setup_time_s"] * 1e3, 3),
+                          "solve_ms": round(r["probe_solve_time_s"] * 1e3, 3), "guarded": r["solve_converged"]}))
 
 
 def timed_seed_start(warmup: int, width: int) -> int:
@@ -567,7 +673,9 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = _args()
-    if a.impl == "reference":
+    if a.kernel is not None:
+        run_kernel(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_native(a)

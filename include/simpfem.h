@@ -275,6 +275,80 @@ int simpfem_pcg_op(int64_t n, simpfem_apply_fn A, simpfem_apply_fn M, void* ctx,
                    double* x, double tol, int maxiter, double* history_host, int history_cap, int* history_len,
                    int* iters, int* converged, void* stream);
 
+/* ---- guarded floor policy, per state and batched -------------------------------
+ * The probe -> preserve/escalate -> floor ladder -> recomputed-true-residual guard of
+ * experiments/phase5/run_gmg_floor_detector_prospective.py:220-354 (_classify :77-90),
+ * run entirely in the library: per attempt E = rho_min + (1 - rho_min) rho^penal on
+ * the device, simpfem_gmg_setup, FGMRES with the hierarchy, and the FP64 guard
+ * ||b - K(E) x|| / ||b|| <= tol.  With a proposer network the decision at the
+ * probe's r50 point follows the learned floor policy (no reference counterpart):
+ * the probe stops there when r50 >= the high threshold (the plain rule raises the
+ * floor whatever r100 shows) or when the network's most probable rung is raised
+ * with probability >= min_confidence; the ladder then starts at that rung (skipped
+ * rungs last, the baseline floor last after a network stop). */
+enum { SIMPFEM_TRIGGER_KEEP = 0, SIMPFEM_TRIGGER_HIGH_R50 = 1, SIMPFEM_TRIGGER_PLATEAU = 2,
+       SIMPFEM_TRIGGER_LEARNED = 3, SIMPFEM_TRIGGER_HIGH_RESIDUAL = 4 };
+typedef struct simpfem_cnn simpfem_cnn;
+typedef struct simpfem_policy_opts {
+  double penal;                       /* 3.0 (the reference drivers default to 4.5) */
+  int binary;                         /* 1: density is a solid mask, void elements take rho = rho_min */
+  double tol;                         /* 1e-6 */
+  int restart, maxiter;               /* 300, 300 */
+  int probe_iters, probe_r50;         /* 100, 50 */
+  double baseline_rho_min;            /* 1e-12 */
+  int n_raised;                       /* 2 (at most 6) */
+  double raised_rho_mins[6];          /* {1e-3, 1e-2} */
+  double high_residual_threshold;     /* 1e-2 */
+  double plateau_residual_threshold;  /* 1e-4 */
+  double plateau_ratio_threshold;     /* 0.6 */
+  int reuse_probe;                    /* 1: a probe that converged on its tolerance at the baseline floor is
+                                         the answer at that floor; 0: re-solved, as the reference driver does */
+  simpfem_cnn* proposer;              /* NULL: the plain probe-and-ladder; else the floor proposer
+                                         (rungs baseline | raised[0], raised[1]) */
+  double min_confidence;              /* 0.5 */
+} simpfem_policy_opts;
+void simpfem_policy_default_opts(simpfem_policy_opts* o);
+
+typedef struct simpfem_policy_result {
+  double probe_r50, probe_r100;       /* r100 NaN when the probe stopped at r50 */
+  int trigger;                        /* SIMPFEM_TRIGGER_* */
+  int raise_floor;                    /* the probe predicted a raised floor */
+  int fallback;                       /* a kept floor failed the guard and the ladder ran */
+  int proposal;                       /* rung proposed at r50 (-1 without a proposer or a check) */
+  double selected_rho_min;            /* the accepted (or last attempted) floor */
+  int converged;                      /* the selected attempt passed the FP64 guard */
+  int reported_converged;             /* FGMRES reported convergence for it */
+  int solve_iters, probe_iters, total_iters, n_setups, n_attempts, reused_probe;
+  double final_rel_residual;          /* guard value of the selected attempt */
+  double attempted[8];                /* floors in attempt order (n_attempts of them) */
+  double seconds;                     /* host wall time of this state, attempts included */
+} simpfem_policy_result;
+
+/* One guarded solve of the state `density` (device, n_elem doubles) with right-hand
+ * side b_free (device, n_free) on hierarchy g; x_free (device, n_free, may be NULL)
+ * receives the selected attempt's solution.  Synchronises `stream` per iteration. */
+int simpfem_policy_run(simpfem_gmg* g, const simpfem_policy_opts* o, const double* density, const double* b_free,
+                       double* x_free, simpfem_policy_result* result, void* stream);
+
+/* A batch of states, possibly of different meshes, solved together on one GPU
+ * (replaces the per-state loop of run_gmg_floor_detector_prospective.py:191-226).
+ * Each state names the hierarchy it is solved on; the hierarchies are the
+ * workers: every worker runs its states in their order on its own stream from
+ * its own host thread, all workers at once, so results depend only on the
+ * assignment (each worker's lambda_max cache carries over between its states as
+ * one driver hierarchy's does).  Distinct hierarchies must sit on distinct mesh
+ * handles (a handle's scratch serves one stream at a time).  With a proposer,
+ * each worker uses its own copy of the network.  The workers start after the
+ * work already queued on `stream` and `stream` waits for all of them. */
+typedef struct simpfem_policy_state {
+  simpfem_gmg* g;
+  const double* density;
+  const double* b_free;
+  double* x_free;                     /* may be NULL */
+} simpfem_policy_state;
+int simpfem_policy_batch(const simpfem_policy_opts* o, const simpfem_policy_state* states, int n_states,
+                         simpfem_policy_result* results, void* stream);
+
 /* Coarsest-level dense factorisation: Linv <- L^{-1}, L the lower Cholesky factor
  * of the SPD row-major n x n device matrix A (A is destroyed; Linv lower with zero
  * upper).  Replaces cp.linalg.cholesky and its finiteness check in
@@ -316,7 +390,6 @@ int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const doub
  * dense 34 -> 3.  Weights are used as bfloat16, everything else float32.
  * Parameters (float32, simpfem_cnn_n_params() of them) in the order
  * W1 b1 W2 b2 W3 b3 W4 b4 Wfc bfc, conv weights [cout][cin][kz][ky][kx]. */
-typedef struct simpfem_cnn simpfem_cnn;
 int simpfem_cnn_n_params(void);
 /* Workspaces for batches of up to max_batch samples; parameters start at zero. */
 int simpfem_cnn_create(int max_batch, simpfem_cnn** out);

@@ -29,14 +29,6 @@ cudaError_t sf_launched(int k) {
 int64_t sf_launch_count() { return g_launches.load(); }
 }  // namespace simpfem
 
-struct simpfem_mesh {
-  Mesh impl;
-};
-struct simpfem_gmg {
-  Gmg* impl = nullptr;
-  simpfem_mesh* mesh = nullptr;
-  DevBuf bfull, xfull;
-};
 
 #define SF_API_BEGIN try {
 #define SF_API_END                                                              \

@@ -320,3 +320,14 @@ void trace_cycle(Gmg& G, const double* rhs_full, int cycle_type, std::vector<dou
                  double* summary);
 
 }  // namespace simpfem
+
+// The C ABI's opaque handles (include/simpfem.h).
+struct simpfem_mesh {
+  simpfem::Mesh impl;
+};
+struct simpfem_gmg {
+  simpfem::Gmg* impl = nullptr;
+  simpfem_mesh* mesh = nullptr;
+  simpfem::DevBuf bfull, xfull;
+};
+

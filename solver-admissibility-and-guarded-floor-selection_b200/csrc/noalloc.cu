@@ -138,10 +138,6 @@ unsigned char* scratch_for_current_device() {
 
 using namespace simpfem;
 
-struct simpfem_mesh {
-  Mesh impl;
-};
-
 extern "C" int simpfem_true_residual_noalloc(simpfem_mesh* mh, const double* E, const double* b_full,
                                              const double* x_full, double* r_full, double* out_host,
                                              void* stream) {

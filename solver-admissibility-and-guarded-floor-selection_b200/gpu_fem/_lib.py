@@ -82,6 +82,55 @@ class GmgProps(ctypes.Structure):
     ]
 
 
+class PolicyOpts(ctypes.Structure):
+    _fields_ = [
+        ("penal", ctypes.c_double),
+        ("binary", ctypes.c_int),
+        ("tol", ctypes.c_double),
+        ("restart", ctypes.c_int),
+        ("maxiter", ctypes.c_int),
+        ("probe_iters", ctypes.c_int),
+        ("probe_r50", ctypes.c_int),
+        ("baseline_rho_min", ctypes.c_double),
+        ("n_raised", ctypes.c_int),
+        ("raised_rho_mins", ctypes.c_double * 6),
+        ("high_residual_threshold", ctypes.c_double),
+        ("plateau_residual_threshold", ctypes.c_double),
+        ("plateau_ratio_threshold", ctypes.c_double),
+        ("reuse_probe", ctypes.c_int),
+        ("proposer", ctypes.c_void_p),
+        ("min_confidence", ctypes.c_double),
+    ]
+
+
+class PolicyResult(ctypes.Structure):
+    _fields_ = [
+        ("probe_r50", ctypes.c_double),
+        ("probe_r100", ctypes.c_double),
+        ("trigger", ctypes.c_int),
+        ("raise_floor", ctypes.c_int),
+        ("fallback", ctypes.c_int),
+        ("proposal", ctypes.c_int),
+        ("selected_rho_min", ctypes.c_double),
+        ("converged", ctypes.c_int),
+        ("reported_converged", ctypes.c_int),
+        ("solve_iters", ctypes.c_int),
+        ("probe_iters", ctypes.c_int),
+        ("total_iters", ctypes.c_int),
+        ("n_setups", ctypes.c_int),
+        ("n_attempts", ctypes.c_int),
+        ("reused_probe", ctypes.c_int),
+        ("final_rel_residual", ctypes.c_double),
+        ("attempted", ctypes.c_double * 8),
+        ("seconds", ctypes.c_double),
+    ]
+
+
+class PolicyState(ctypes.Structure):
+    _fields_ = [("g", ctypes.c_void_p), ("density", ctypes.c_void_p), ("b_free", ctypes.c_void_p),
+                ("x_free", ctypes.c_void_p)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -120,6 +169,9 @@ _SIGS = {
     "simpfem_fgmres_op": (_I, [_I64, _P, _P, _P, _P, _P, _P, _D, _I, _I, _P, _I, _P, _P, _P, _P]),
     "simpfem_pcg_op": (_I, [_I64, _P, _P, _P, _P, _P, _P, _D, _I, _P, _I, _P, _P, _P, _P]),
     "simpfem_dense_cholesky_inverse": (_I, [_I, _P, _P, _P, _P]),
+    "simpfem_policy_default_opts": (None, [_P]),
+    "simpfem_policy_run": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "simpfem_policy_batch": (_I, [_P, _P, _I, _P, _P]),
     "simpfem_cone_filter": (_I, [_I, _I, _I, _D, _I, _P, _P, _P]),
     "simpfem_oc_work_bytes": (ctypes.c_size_t, []),
     "simpfem_oc_update": (_I, [_I64, _P, _P, _P, _P, _D, _D, _P, _P, ctypes.c_size_t, _P, _P, _P, _P]),

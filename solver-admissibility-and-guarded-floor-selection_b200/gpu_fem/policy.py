@@ -15,6 +15,7 @@ recomputed from x after the solve.
 
 from __future__ import annotations
 
+import ctypes
 import threading
 import time
 from dataclasses import dataclass, field
@@ -228,6 +229,71 @@ class GuardedFloorPolicy:
         }
 
 
+_TRIGGERS = ("keep", "high_r50", "plateau", "learned", "high_residual")
+
+
+def native_opts(pol: "GuardedFloorPolicy", *, binary: bool = False) -> "_lib.PolicyOpts":
+    """The library's policy options (simpfem_policy_opts) of a GuardedFloorPolicy or
+    LearnedFloorPolicy."""
+    if pol.severity_jump_r50_threshold > 0.0 or pol.checkpoint_guard:
+        raise ValueError("the severity jump and the checkpointed guard run in the Python policy only")
+    if len(pol.raised_rho_mins) > 6:
+        raise ValueError("at most six raised floors")
+    o = _lib.PolicyOpts()
+    _lib.lib().simpfem_policy_default_opts(ctypes.byref(o))
+    o.penal = pol.penal
+    o.binary = int(bool(binary))
+    o.tol = pol.tol
+    o.restart, o.maxiter = pol.restart, pol.maxiter
+    o.probe_iters, o.probe_r50 = pol.probe_iters, pol.probe_r50
+    o.baseline_rho_min = pol.baseline_rho_min
+    o.n_raised = len(pol.raised_rho_mins)
+    for k, v in enumerate(pol.raised_rho_mins):
+        o.raised_rho_mins[k] = v
+    o.high_residual_threshold = pol.thresholds["high_residual_threshold"]
+    o.plateau_residual_threshold = pol.thresholds["plateau_residual_threshold"]
+    o.plateau_ratio_threshold = pol.thresholds["plateau_ratio_threshold"]
+    o.reuse_probe = int(bool(pol.reuse_probe))
+    proposer = getattr(pol, "proposer", None)
+    if proposer is not None:
+        o.proposer = proposer._h.value
+        o.min_confidence = pol.min_confidence
+    return o
+
+
+def native_row(r: "_lib.PolicyResult") -> dict:
+    """A result row of the library's policy, with the keys of GuardedFloorPolicy.run."""
+    attempted = [r.attempted[k] for k in range(r.n_attempts)]
+    trig = _TRIGGERS[r.trigger]
+    return {
+        "probe_r50": r.probe_r50, "probe_r100": r.probe_r100, "probe_iters": r.probe_iters, "trigger": trig,
+        "predicted_raise_floor": r.raise_floor, "post_solve_fallback_triggered": r.fallback,
+        "detector_false_keep": int((not r.raise_floor) and r.fallback),
+        "stopped_at_r50": trig if trig in ("learned", "high_residual") else "", "proposal": r.proposal,
+        "recommended_rho_min": r.selected_rho_min, "attempted_rho_mins": ";".join(f"{v:.0e}" for v in attempted),
+        "n_floor_attempts": r.n_attempts, "solve_converged": r.converged,
+        "solver_reported_converged": r.reported_converged, "solve_iters": r.solve_iters,
+        "solve_final_rel_residual": r.final_rel_residual, "selected_reused_probe": r.reused_probe,
+        "n_setups": r.n_setups, "total_iters": r.total_iters, "policy_time_s": r.seconds,
+    }
+
+
+def run_native(pol: "GuardedFloorPolicy", density, *, binary: bool = False) -> dict:
+    """One guarded solve of ``density`` run entirely in the library (simpfem_policy_run)
+    on the current stream; the same decisions and kernels as ``pol.run`` (the guard
+    value may differ in its last bits: the library reduces in its fixed order).
+    The solution is left in ``pol.last_x``."""
+    torch = _lib.require_cuda()
+    d = _lib.as_cuda(density, torch.float64)
+    x = torch.empty_like(pol.F_free_gpu)
+    res = _lib.PolicyResult()
+    o = native_opts(pol, binary=binary)
+    _lib.call("simpfem_policy_run", pol.gmg._h, ctypes.byref(o), _lib.ptr(d), _lib.ptr(pol.F_free_gpu), _lib.ptr(x),
+              ctypes.byref(res), _lib.stream_ptr())
+    pol.last_x = x
+    return native_row(res)
+
+
 class BatchedFloorPolicy:
     """Several density states in flight at once on one GPU.
 
@@ -266,6 +332,28 @@ class BatchedFloorPolicy:
         # grid) then reuses them
         _lib.call("simpfem_mesh_tune", self.workers[0].mf_op.mesh.handle, _lib.stream_ptr())
         torch.cuda.current_stream().synchronize()
+
+    def run_many_native(self, densities, *, binary: bool = False, keep_x: bool = True) -> list:
+        """run_many in the library (simpfem_policy_batch): state k goes to worker
+        k mod width, each worker's states in order on its own stream and host thread
+        inside the library, so the rows (and solutions) are those of run_many.  With
+        ``keep_x`` the solutions are in ``self.last_xs`` (one device tensor per state)."""
+        torch = _lib.require_cuda()
+        n = len(densities)
+        dens = [_lib.as_cuda(d, torch.float64) for d in densities]
+        xs = [torch.empty_like(self.workers[k % self.width].F_free_gpu) for k in range(n)] if keep_x else []
+        states = (_lib.PolicyState * max(n, 1))()
+        for k in range(n):
+            w = self.workers[k % self.width]
+            states[k].g = w.gmg._h.value
+            states[k].density = _lib.ptr(dens[k])
+            states[k].b_free = _lib.ptr(w.F_free_gpu)
+            states[k].x_free = _lib.ptr(xs[k]) if keep_x else None
+        results = (_lib.PolicyResult * max(n, 1))()
+        o = native_opts(self.workers[0], binary=binary)
+        _lib.call("simpfem_policy_batch", ctypes.byref(o), states, n, results, _lib.stream_ptr())
+        self.last_xs = xs
+        return [native_row(results[k]) for k in range(n)]
 
     def run_many(self, densities, *, binary: bool = False, on_result=None) -> list:
         """Run the policy on every state; returns the result rows in input order.

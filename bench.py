@@ -67,8 +67,12 @@ def _args():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--stack", default="plain", choices=["plain", "canonical"])
     ap.add_argument("--width", type=int, default=8, help="states in flight per GPU in the mixed arm")
-    ap.add_argument("--policy", default="learned", choices=["learned", "plain"],
-                    help="mixed arm: learned floor proposal (decides at r50) or the plain probe-and-ladder")
+    ap.add_argument("--policy", default="learned", choices=["learned", "plain", "rule"],
+                    help="mixed arm: learned floor proposal (decides at r50), the plain probe-and-ladder, or "
+                         "the r50 rule stop alone")
+    ap.add_argument("--workload", default="filtered", choices=["filtered", "escalating"],
+                    help="filtered: the workload's states; escalating: unfiltered masks, void p 0.5-0.7, whose "
+                         "probes escalate")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # single-kernel launches for timing and ncu captures (no bench line)
     ap.add_argument("--kernel", default=None, choices=["smoother-step", "operator", "dense", "policy"],
@@ -215,7 +219,16 @@ def _filter():
     return _build_density_filter(NX, NY, 1.5, NZ)
 
 
-def make_state(H, seed: int) -> np.ndarray:
+ESCALATING_PROBS = (0.5, 0.6, 0.7)
+
+
+def make_state(H, seed: int, workload: str = "filtered") -> np.ndarray:
+    """The workload's state: void with probability PROBS[seed % 3], cone filter
+    r = 1.5; ``escalating``: unfiltered solid masks with void probability
+    ESCALATING_PROBS[seed % 3], where the probe's r50 / r100 rule raises floors."""
+    if workload == "escalating":
+        p = ESCALATING_PROBS[seed % len(ESCALATING_PROBS)]
+        return (np.random.default_rng(seed).random(NX * NY * NZ) >= p).astype(np.float64)
     p = PROBS[seed % len(PROBS)]
     solid = (np.random.default_rng(seed).random(NX * NY * NZ) >= p).astype(np.float64)
     return np.asarray(H @ solid)
@@ -343,7 +356,7 @@ def run_native(args):
     K, W, B = args.steps, args.warmup, max(1, args.width)
     WB = timed_seed_start(W, B)  # warm-up states for the batched arm: every worker sees at least two
     seeds = rank_seeds(rank, WB + 2 * K)
-    states = {s: make_state(H, s) for s in seeds}
+    states = {s: make_state(H, s, args.workload) for s in seeds}
 
     def policy_kwargs(precision):
         return dict(penal=3.0, tol=1e-6, restart=300, maxiter=300, probe_iters=100, probe_r50=50,
@@ -412,6 +425,8 @@ def run_native(args):
         from gpu_fem.floor_proposer import DEFAULT_WEIGHTS
 
         learned = DEFAULT_WEIGHTS
+    elif args.policy == "rule":
+        learned = "rule"
     mixed = BatchedFloorPolicy(B, spec, learned=learned, **policy_kwargs("mixed"))
     mixed.run_many([torch.as_tensor(states[s], device="cuda") for s in seeds[:WB]])
     timed_seeds = seeds[WB:WB + K]
@@ -488,7 +503,9 @@ def run_native(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 V-cycle (bf16-stored coarse stencils), f64 FGMRES/Cholesky/guard",
-        "data": "synthetic (seeded void p in {0.2,0.35,0.5}, cone filter r=1.5, SIMP p=3)",
+        "data": ("synthetic (seeded void p in {0.2,0.35,0.5}, cone filter r=1.5, SIMP p=3)"
+                 if args.workload == "filtered" else
+                 "synthetic escalating (seeded unfiltered masks, void p in {0.5,0.6,0.7}, SIMP p=3)"),
         "config": {
             "workload": "guarded SIMP-floor solve, cantilever 160x80x40 (512,000 elements, "
                         f"{n_free} free DOFs), floors 1e-12|1e-3,1e-2, 4-level GMG ({args.stack} stack), "
@@ -535,6 +552,9 @@ def run_native(args):
             "note": "mixed vs FP64 solve of the same state, both stopped at true relative residual <= 1e-6",
         },
         "policy": args.policy,
+        "workload": args.workload,
+        "triggers": {t: sum(1 for r in rows_mixed if r["trigger"] == t) for t in sorted({r["trigger"] for r in rows_mixed})},
+        "mixed_total_outer_iterations": int(sum(r["total_iters"] for r in rows_mixed)),
         "learned_stops_at_r50": sum(1 for r in rows_mixed + rows_e2e if r.get("stopped_at_r50")),
         "e2e": {
             "value": round(e2e_value, 4),
@@ -657,7 +677,7 @@ def run_reference(args):
     first = timed_seed_start(args.warmup, args.width)
     times = []
     for i in range(steps):
-        d = make_state(H, first + i)
+        d = make_state(H, first + i, args.workload)
         t0 = time.perf_counter()
         run_state(op, g, Ff, lambda rm, d=d: d, penal=3.0, raised=(1e-3, 1e-2), restart=300, maxiter=300)
         times.append(time.perf_counter() - t0)

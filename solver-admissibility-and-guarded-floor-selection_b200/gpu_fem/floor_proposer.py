@@ -74,6 +74,7 @@ class FloorProposerNet:
         _lib.call("simpfem_cnn_create", self.max_batch, ctypes.byref(h))
         self._h = h
         self.set_params(he_init(seed, self.n_params) if params is None else params)
+        self.min_confidence = 0.5
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -179,8 +180,13 @@ class FloorProposerNet:
 
     @classmethod
     def load(cls, path: str = DEFAULT_WEIGHTS, max_batch: int = 256) -> "FloorProposerNet":
+        """The network saved at ``path``; its ``min_confidence`` is the threshold
+        calibrated with it (0.5 when the file holds none)."""
         with np.load(path) as z:
-            return cls(max_batch=max_batch, params=z["params"])
+            net = cls(max_batch=max_batch, params=z["params"])
+            if "min_confidence" in z.files:
+                net.min_confidence = float(z["min_confidence"])
+            return net
 
 
 class LearnedFloorPolicy(GuardedFloorPolicy):
@@ -188,13 +194,14 @@ class LearnedFloorPolicy(GuardedFloorPolicy):
 
     ``proposer`` is a FloorProposerNet; ``dims`` the element grid of the preset
     (for pooling); ``min_confidence``: proposals whose softmax probability is
-    below it count as rung 0 (the probe continues and the plain rule decides).
+    below it count as rung 0 (the probe continues and the plain rule decides);
+    None takes the threshold calibrated with the network (``proposer.min_confidence``).
     Attempt order after a stop at r50: the proposed rung (at least 1e-3), the
     raised rungs above it, the raised rungs below it, and -- when the stop was the
     proposer's and not the high-residual rule's -- the baseline floor last."""
 
     def __init__(self, preset, *, proposer: FloorProposerNet, dims: Optional[Sequence[int]] = None,
-                 min_confidence: float = 0.5, **kwargs):
+                 min_confidence: Optional[float] = None, **kwargs):
         super().__init__(preset, **kwargs)
         if dims is None:
             dims = (self.spec.nelx, self.spec.nely, self.spec.nelz)
@@ -205,7 +212,7 @@ class LearnedFloorPolicy(GuardedFloorPolicy):
             raise ValueError("the severity jump is not combined with the learned proposal")
         self.proposer = proposer
         self.dims = tuple(int(d) for d in dims)
-        self.min_confidence = float(min_confidence)
+        self.min_confidence = float(proposer.min_confidence if min_confidence is None else min_confidence)
 
     # device steps of the decision (a host test replaces them)
     def _pool(self, density):

@@ -308,7 +308,9 @@ class BatchedFloorPolicy:
 
     ``learned``: path of floor-proposer weights (gpu_fem.floor_proposer); the
     workers are then LearnedFloorPolicy instances, each with its own network
-    handle (a handle's workspaces serve one stream at a time).
+    handle (a handle's workspaces serve one stream at a time).  "rule": the same
+    workers with a network of zeros, i.e. the probe stops at r50 only on the
+    plain rule's high-residual trigger.
     """
 
     def __init__(self, width: int = 3, *args, learned: Optional[str] = None, **kwargs):
@@ -325,7 +327,12 @@ class BatchedFloorPolicy:
                 else:
                     from .floor_proposer import FloorProposerNet, LearnedFloorPolicy
 
-                    net = FloorProposerNet.load(learned, max_batch=1)
+                    if learned == "rule":
+                        # a network of zeros proposes no raised rung: the r50 rule stop alone
+                        net = FloorProposerNet(max_batch=1)
+                        net.set_params(np.zeros(net.n_params, dtype=np.float32))
+                    else:
+                        net = FloorProposerNet.load(learned, max_batch=1)
                     self.workers.append(LearnedFloorPolicy(*args, proposer=net, **kwargs))
         self.streams = [torch.cuda.Stream() for _ in range(self.width)]
         # pick the sweep shapes now, on an idle device; every worker's mesh (same

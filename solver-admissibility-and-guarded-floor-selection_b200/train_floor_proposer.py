@@ -20,6 +20,15 @@ LearnedFloorPolicy, and compared: floor attempts, setups, outer iterations,
 policy time, selected floor, guarded answers.  Writes
 floor_proposer.npz (parameters) and floor_proposer_eval.json (dataset, training
 curve, held-out comparison).
+
+    python train_floor_proposer.py --calibrate 256
+
+keeps the saved network and picks its confidence threshold (the softmax
+probability below which a proposal counts as "keep the probe running") on 256
+fresh states: the threshold with the fewest outer iterations among those that
+guard as many answers as the plain policy.  It is saved with the parameters
+(LearnedFloorPolicy uses it by default) and the held-out states are compared
+again with it.
 """
 
 from __future__ import annotations
@@ -139,6 +148,39 @@ def evaluate(net, held):
     return rows
 
 
+def calibrate(net, states, thresholds):
+    """Total outer iterations and guarded answers of the plain policy, the r50 rule
+    stop alone and the learned policy at each confidence threshold on ``states``
+    (one state at a time, as in ``evaluate``)."""
+    import torch
+
+    from gpu_fem.floor_proposer import FloorProposerNet, LearnedFloorPolicy
+    from gpu_fem.policy import GuardedFloorPolicy
+    from gpu_fem.presets import cantilever_spec
+
+    zero = FloorProposerNet(max_batch=4, params=np.zeros(net.n_params, dtype=np.float32))
+    arms = ["plain", "rule"] + [f"learned@{t:g}" for t in thresholds]
+    tot = {a: {"outer_iterations": 0, "guarded": 0, "same_floor_as_plain": 0} for a in arms}
+    for dims in MESHES:
+        idx = [i for i, st in enumerate(states) if st["dims"] == dims]
+        if not idx:
+            continue
+        spec = cantilever_spec(*dims)
+        pols = {"plain": GuardedFloorPolicy(spec, stack=_stack(), **POLICY),
+                "rule": LearnedFloorPolicy(spec, proposer=zero, dims=dims, stack=_stack(), **POLICY)}
+        for t in thresholds:
+            pols[f"learned@{t:g}"] = LearnedFloorPolicy(spec, proposer=net, dims=dims, min_confidence=t,
+                                                        stack=_stack(), **POLICY)
+        for i in idx:
+            d = torch.as_tensor(states[i]["density"], device="cuda")
+            rows = {a: pol.run(d) for a, pol in pols.items()}
+            for a, r in rows.items():
+                tot[a]["outer_iterations"] += int(r["total_iters"])
+                tot[a]["guarded"] += int(r["solve_converged"])
+                tot[a]["same_floor_as_plain"] += int(r["recommended_rho_min"] == rows["plain"]["recommended_rho_min"])
+    return tot
+
+
 def compare(rows, mask=None):
     """Totals per policy over the states in ``mask`` (all by default); floors are
     compared with the plain policy's selection."""
@@ -173,10 +215,45 @@ def main() -> None:
     ap.add_argument("--val", type=int, default=512)
     ap.add_argument("--width", type=int, default=4)
     ap.add_argument("--out", default=os.path.join(HERE, "gpu_fem", "data"))
+    ap.add_argument("--calibrate", type=int, default=0, metavar="N",
+                    help="only calibrate the saved network's confidence threshold on N fresh states "
+                         "(seed 2) and re-evaluate the held-out states with it")
     a = ap.parse_args()
     import torch
 
     from gpu_fem.floor_proposer import FloorProposerNet
+
+    if a.calibrate:
+        path = os.path.join(a.out, "floor_proposer.npz")
+        net = FloorProposerNet.load(path, max_batch=4)
+        thresholds = (0.5, 0.7, 0.9, 0.97, 0.995)
+        cal = calibrate(net, make_states(a.calibrate, seed=2), thresholds)
+        # the threshold with the fewest outer iterations among those guarding as many
+        # answers as the plain policy; ties go to the higher (more conservative) one
+        ok = [t for t in thresholds if cal[f"learned@{t:g}"]["guarded"] >= cal["plain"]["guarded"]]
+        best = min(ok, key=lambda t: (cal[f"learned@{t:g}"]["outer_iterations"], -t)) if ok else 1.0
+        net.min_confidence = float(best)
+        held = make_states(a.heldout, seed=1)
+        rows = evaluate(net, held)
+        escalated = [r["predicted_raise_floor"] == 1 or r["n_floor_attempts"] > 1 for r in rows["plain"]]
+        with open(os.path.join(a.out, "floor_proposer_eval.json")) as fh:
+            summary = json.load(fh)
+        summary["calibration"] = {"states": a.calibrate, "seed": 2, "thresholds": list(thresholds),
+                                  "totals": cal, "chosen_min_confidence": best}
+        summary["heldout_policies_calibrated"] = {
+            "min_confidence": best,
+            "all": compare(rows),
+            "plain_escalated": compare(rows, escalated),
+            "plain_kept": compare(rows, [not e for e in escalated]),
+        }
+        with np.load(path) as z:
+            meta = {k: z[k] for k in z.files if k not in ("params", "min_confidence")}
+        net.save(path, min_confidence=best, **meta)
+        with open(os.path.join(a.out, "floor_proposer_eval.json"), "w") as fh:
+            json.dump(summary, fh, indent=1)
+        print(json.dumps({"calibration": summary["calibration"],
+                          "heldout": summary["heldout_policies_calibrated"]}, indent=1))
+        return
 
     t0 = time.time()
     train = make_states(a.train, seed=0)

@@ -70,6 +70,8 @@ def _args():
     ap.add_argument("--policy", default="learned", choices=["learned", "plain", "rule"],
                     help="mixed arm: learned floor proposal (decides at r50), the plain probe-and-ladder, or "
                          "the r50 rule stop alone")
+    ap.add_argument("--batch", default="threads", choices=["threads", "native"],
+                    help="mixed arm: workers driven from Python threads, or the library's batch entry")
     ap.add_argument("--workload", default="filtered", choices=["filtered", "escalating"],
                     help="filtered: the workload's states; escalating: unfiltered masks, void p 0.5-0.7, whose "
                          "probes escalate")
@@ -411,7 +413,13 @@ def run_native(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = _lib.lib().simpfem_launch_count()
         e0.record()
-        rows = bp.run_many(dens, on_result=keep_x if host_io else None)
+        if args.batch == "native":
+            # the whole batch inside the library (simpfem_policy_batch); solutions copied after
+            rows = bp.run_many_native(dens, keep_x=host_io)
+            for k in range(len(xs)):
+                xs[k].copy_(bp.last_xs[k], non_blocking=True)
+        else:
+            rows = bp.run_many(dens, on_result=keep_x if host_io else None)
         e1.record()
         barrier()
         ms = e0.elapsed_time(e1)
@@ -512,7 +520,7 @@ def run_native(args):
                         "FGMRES restart 300 tol 1e-6, r50/r100 probe 100 its",
             "global_batch": n_states,
             "batch_width": B,
-            "parallelism": f"{B} states in flight per GPU (one stream each) x {world} replicas",
+            "parallelism": f"{B} states in flight per GPU (one stream each, {args.batch}) x {world} replicas",
             "l2": "working set larger than L2 (FGMRES basis + hierarchy > 126 MB); no flush",
         },
         "clocks": clk.summary(),

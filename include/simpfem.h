@@ -383,6 +383,27 @@ int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const doub
                       double volfrac, double move, double* rho_new, double* work, size_t work_bytes,
                       double* change_host, double* lambda_host, int* steps_host, void* stream);
 
+/* Heaviside projection proj = (tanh(b eta) + tanh(b (x - eta))) / den and its
+ * derivative dproj = b (1 - tanh(b (x - eta))^2) / den, den = tanh(b eta) +
+ * tanh(b (1 - eta)) (_heaviside / _heaviside_deriv, pub_simp_solver.py:245-253);
+ * x, proj, dproj: device arrays of n doubles (proj or dproj may be NULL); beta > 0. */
+int simpfem_heaviside(int64_t n, const double* x, double beta, double eta, double* proj, double* dproj,
+                      void* stream);
+/* Bytes of device workspace simpfem_oc_update_projected needs for n elements. */
+size_t simpfem_oc_projected_work_bytes(int64_t n);
+/* The OC update with the Heaviside projection (_oc_step_cupy with use_heaviside and
+ * beta > 1e-6, simp_gpu.py:245-290): dh = the projection's derivative at rho_f,
+ * design sensitivities H^T (dc_phys dh) and H^T dh with the cone filter of radius
+ * rmin on the nx x ny x nz grid, then the bisection (at most 100 steps, bracket
+ * < 1e-9) of rn against the projected filtered volume
+ * sum(tanh(b eta) + tanh(b (H rn - eta))) / den = volfrac n.  rho, rho_f, dc_phys,
+ * rho_new: device arrays of nx ny nz doubles; work: at least
+ * simpfem_oc_projected_work_bytes(n) bytes.  Synchronises the stream once per step. */
+int simpfem_oc_update_projected(int nx, int ny, int nz, double rmin, const double* rho, const double* rho_f,
+                                const double* dc_phys, double beta, double eta, double volfrac, double move,
+                                double* rho_new, double* work, size_t work_bytes, double* change_host,
+                                double* lambda_host, int* steps_host, void* stream);
+
 /* ---- learned floor proposer (no counterpart in the reference) ------------------
  * A small 3D CNN over the density pooled to 16^3 plus two probe features, with a
  * 3-way softmax over the floor rungs {1e-12, 1e-3, 1e-2}: conv 1->16 (stride 1),

@@ -517,7 +517,7 @@ static bool x2_shape_ok(const Grid& g, const SweepShape& sh) {
 template <int EPI>
 static cudaError_t launch_sweep_f32(const Grid& g, const SweepShape& sh, const float* E, const uint8_t* mask,
                                     const float* u, const EpiArgs& ea, cudaStream_t s) {
-  if (!x2_shape_ok(g, sh)) return launch_sweep<float, EPI, 0, 512>(g, sh, E, mask, u, ea, s);
+  if (sh.one || !x2_shape_ok(g, sh)) return launch_sweep<float, EPI, 0, 512>(g, sh, E, mask, u, ea, s);
   const int NT = sh.bj * sh.bk / 2, NE = sh.bj * sh.bk;
   const size_t smem = sizeof(float) * (36 * (size_t)NE + 9 * (size_t)(sh.bj + 1) * (sh.bk + 2));
   static bool attr_done = false;

@@ -228,6 +228,13 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
         sh.bk = bk;
         sh.cx = cx;
         cands.push_back(sh);
+        // FP32: the one-element-per-thread sweep as well; it has twice the threads
+        // of the packed sweep for the same tile, which can hide more latency on grids
+        // too small to fill the GPU with packed blocks
+        if (t == F32) {
+          sh.one = 1;
+          cands.push_back(sh);
+        }
       }
     }
   cudaEvent_t e0, e1;
@@ -254,8 +261,8 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
     float ms = 0.f;
     SF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     if (verbose)
-      fprintf(stderr, "[simpfem tune] %s %dx%dx%d bj=%d bk=%d cx=%d: %.1f us\n", t == F64 ? "f64" : "f32", m.g.nx,
-              m.g.ny, m.g.nz, sh.bj, sh.bk, sh.cx, ms * 1000.f / 3.f);
+      fprintf(stderr, "[simpfem tune] %s %dx%dx%d bj=%d bk=%d cx=%d one=%d: %.1f us\n", t == F64 ? "f64" : "f32",
+              m.g.nx, m.g.ny, m.g.nz, sh.bj, sh.bk, sh.cx, sh.one, ms * 1000.f / 3.f);
     if (ms < best) {
       best = ms;
       best_sh = sh;

@@ -60,6 +60,8 @@ struct SweepShape {
   int bj = 8;   // element columns along y per block (one of them is a halo column)
   int bk = 32;  // element columns along z per block (one halo column)
   int cx = 8;   // node planes along x per block
+  int one = 0;  // FP32: 1 = one element per thread (the scalar sweep) even where the
+                // two-element packed sweep applies; picked by the tuner like the tile
 };
 
 struct WhtBlocks {

@@ -127,6 +127,33 @@ __global__ void oc_finish_kernel(int nb, int mode, const double* __restrict__ pa
   *out = s;
 }
 
+// Heaviside projection of x and its derivative (pub_simp_solver.py:245-253):
+// p = (tanh(b eta) + tanh(b (x - eta))) / den, dp = b (1 - tanh(b (x - eta))^2) / den,
+// den = tanh(b eta) + tanh(b (1 - eta)); dc (optional) is multiplied by dp into dcdp.
+__global__ void heaviside_kernel(int64_t n, const double* __restrict__ x, double beta, double eta, double tbe,
+                                 double den, double* __restrict__ p, double* __restrict__ dp,
+                                 const double* __restrict__ dc, double* __restrict__ dcdp) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const double t = tanh(beta * (x[e] - eta));
+  if (p) p[e] = (tbe + t) / den;
+  const double d = beta * (1.0 - t * t) / den;
+  if (dp) dp[e] = d;
+  if (dcdp) dcdp[e] = dc[e] * d;
+}
+
+// partial sums of tanh(b eta) + tanh(b (x - eta)) (the projected volume times den)
+__global__ void __launch_bounds__(kSimpThreads) projected_sum_kernel(int64_t n, const double* __restrict__ x,
+                                                                     double beta, double eta, double tbe,
+                                                                     double* __restrict__ partials) {
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    v += tbe + tanh(beta * (x[e] - eta));
+  const double t = block_reduce_sum(v, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
 FilterOffsets make_offsets(double rmin) {
   FilterOffsets o{};
   const int r = (int)floor(rmin);
@@ -238,6 +265,84 @@ int simpfem_oc_update(int64_t n, const double* rho, const double* dc, const doub
     if (l2 - l1 < 1e-9) break;
   }
   oc_pass_kernel<<<nb, kSimpThreads, 0, s>>>(n, rho, dc, dv, vol_w, lm, move, 1, rho_new, partials);
+  oc_finish_kernel<<<1, 32, 0, s>>>(nb, 1, partials, out);
+  SF_CUDA(sf_launched(2));
+  double ch = 0.0;
+  SF_CUDA(cudaMemcpyAsync(&ch, out, sizeof(double), cudaMemcpyDeviceToHost, s));
+  SF_CUDA(cudaStreamSynchronize(s));
+  if (change_host) *change_host = ch;
+  if (lambda_host) *lambda_host = lm;
+  if (steps_host) *steps_host = steps;
+  SIMP_API_END
+}
+
+int simpfem_heaviside(int64_t n, const double* x, double beta, double eta, double* proj, double* dproj,
+                      void* stream) {
+  SIMP_API_BEGIN
+  if (n < 1 || !x || (!proj && !dproj)) throw InvalidArg{"simpfem_heaviside: bad argument"};
+  if (!(beta > 0.0)) throw InvalidArg{"simpfem_heaviside: beta must be positive"};
+  const double tbe = tanh(beta * eta), den = tbe + tanh(beta * (1.0 - eta));
+  cudaStream_t s = (cudaStream_t)stream;
+  heaviside_kernel<<<div_up(n, 256), 256, 0, s>>>(n, x, beta, eta, tbe, den, proj, dproj, nullptr, nullptr);
+  SF_CUDA(sf_launched(1));
+  SIMP_API_END
+}
+
+size_t simpfem_oc_projected_work_bytes(int64_t n) {
+  return sizeof(double) * (5 * (size_t)std::max<int64_t>(n, 1) + kSimpBlocks + 2);
+}
+
+int simpfem_oc_update_projected(int nx, int ny, int nz, double rmin, const double* rho, const double* rho_f,
+                                const double* dc_phys, double beta, double eta, double volfrac, double move,
+                                double* rho_new, double* work, size_t work_bytes, double* change_host,
+                                double* lambda_host, int* steps_host, void* stream) {
+  SIMP_API_BEGIN
+  const int64_t n = (int64_t)nx * ny * nz;
+  if (nx < 1 || ny < 1 || nz < 1 || !rho || !rho_f || !dc_phys || !rho_new || !work)
+    throw InvalidArg{"simpfem_oc_update_projected: null argument"};
+  if (work_bytes < simpfem_oc_projected_work_bytes(n))
+    throw InvalidArg{"simpfem_oc_update_projected: workspace too small"};
+  if (!(beta > 1e-6)) throw InvalidArg{"simpfem_oc_update_projected: beta must exceed 1e-6 (else simpfem_oc_update)"};
+  if (!(rmin >= 1.0 && rmin <= 3.5)) throw InvalidArg{"simpfem_oc_update_projected: rmin must be in [1, 3.5]"};
+  cudaStream_t s = (cudaStream_t)stream;
+  set_filter(rmin, s);
+  double* dh = work;
+  double* dcdh = dh + n;  // dc * dh, then reused for the filtered candidate
+  double* dcd = dcdh + n;
+  double* dvd = dcd + n;
+  double* rn = dvd + n;
+  double* partials = rn + n;
+  double* out = partials + kSimpBlocks;
+  const double tbe = tanh(beta * eta), den = tbe + tanh(beta * (1.0 - eta));
+  const int eb = div_up(n, 256);
+  // sensitivities in the design space (simp_gpu.py:245-258): H^T (dc dh), H^T dh
+  heaviside_kernel<<<eb, 256, 0, s>>>(n, rho_f, beta, eta, tbe, den, nullptr, dh, dc_phys, dcdh);
+  cone_filter_kernel<<<eb, 256, 0, s>>>(nx, ny, nz, 1, dcdh, dcd);
+  cone_filter_kernel<<<eb, 256, 0, s>>>(nx, ny, nz, 1, dh, dvd);
+  SF_CUDA(sf_launched(3));
+  double* rnf = dcdh;
+  const int nb = (int)std::min<int64_t>(kSimpBlocks, div_up(n, kSimpThreads));
+  const double target = volfrac * (double)n;
+  double l1 = 0.0, l2 = 1e9, lm = 0.5 * (l1 + l2);
+  int steps = 0;
+  // the bisection of simp_gpu.py:268-290 with the projected volume of each candidate:
+  // sum(tanh(b eta) + tanh(b (H rn - eta))) / den against volfrac n
+  for (int it = 0; it < 100; ++it) {
+    lm = 0.5 * (l1 + l2);
+    oc_pass_kernel<<<nb, kSimpThreads, 0, s>>>(n, rho, dcd, dvd, nullptr, lm, move, 1, rn, partials);
+    cone_filter_kernel<<<eb, 256, 0, s>>>(nx, ny, nz, 0, rn, rnf);
+    projected_sum_kernel<<<nb, kSimpThreads, 0, s>>>(n, rnf, beta, eta, tbe, partials);
+    oc_finish_kernel<<<1, 32, 0, s>>>(nb, 0, partials, out);
+    SF_CUDA(sf_launched(4));
+    double vol = 0.0;
+    SF_CUDA(cudaMemcpyAsync(&vol, out, sizeof(double), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    ++steps;
+    if (vol / den > target) l1 = lm;
+    else l2 = lm;
+    if (l2 - l1 < 1e-9) break;
+  }
+  oc_pass_kernel<<<nb, kSimpThreads, 0, s>>>(n, rho, dcd, dvd, nullptr, lm, move, 1, rho_new, partials);
   oc_finish_kernel<<<1, 32, 0, s>>>(nb, 1, partials, out);
   SF_CUDA(sf_launched(2));
   double ch = 0.0;

@@ -175,6 +175,10 @@ _SIGS = {
     "simpfem_cone_filter": (_I, [_I, _I, _I, _D, _I, _P, _P, _P]),
     "simpfem_oc_work_bytes": (ctypes.c_size_t, []),
     "simpfem_oc_update": (_I, [_I64, _P, _P, _P, _P, _D, _D, _P, _P, ctypes.c_size_t, _P, _P, _P, _P]),
+    "simpfem_heaviside": (_I, [_I64, _P, _D, _D, _P, _P, _P]),
+    "simpfem_oc_projected_work_bytes": (ctypes.c_size_t, [_I64]),
+    "simpfem_oc_update_projected": (_I, [_I, _I, _I, _D, _P, _P, _P, _D, _D, _D, _D, _P, _P, ctypes.c_size_t, _P, _P,
+                                         _P, _P]),
     "simpfem_cnn_n_params": (_I, []),
     "simpfem_cnn_create": (_I, [_I, ctypes.POINTER(_P)]),
     "simpfem_cnn_destroy": (_I, [_P]),

@@ -258,30 +258,50 @@ def test_wrong_proposal_stays_guarded(cuda):
 
 
 def test_trained_proposer_gains_over_plain_policy(cuda):
-    """The committed network (gpu_fem/data/floor_proposer.npz) against the plain
-    probe-and-ladder on states it was not trained on: unfiltered masks over the
-    void fractions where escalations occur plus filtered fields.  Every answer the
-    plain policy guards is guarded, the learned policy needs fewer outer
-    iterations in total, and it selects the plain policy's floor on most states.
-    The r50 rule stop without the network is reported beside it."""
-    from gpu_fem.floor_proposer import DEFAULT_WEIGHTS, FloorProposerNet
+    """The committed network (gpu_fem/data/floor_proposer.npz, with the confidence
+    threshold calibrated on fresh states) against the plain probe-and-ladder and
+    against the r50 rule stop without the network, on the first 128 held-out
+    states of the training script's generator (seed 1: half cone-filtered, half
+    unfiltered masks, 40x20x20 and 80x40x20): every answer the plain policy guards
+    is guarded, the learned policy needs fewer outer iterations than the plain one,
+    no more than the rule stop alone (2 % slack on this subset; on all 512 held-out
+    states it needs 1.7 % fewer, floor_proposer_eval.json), and selects the plain
+    policy's floor on at least 95 % of the states."""
+    import os
+    import sys
+
+    from gpu_fem.floor_proposer import DEFAULT_WEIGHTS, FloorProposerNet, LearnedFloorPolicy
+    from gpu_fem.paper4 import PLAIN_JACOBI_STACK
+    from gpu_fem.policy import GuardedFloorPolicy
+    from gpu_fem.presets import cantilever_spec
+
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "solver-admissibility-and-guarded-floor-selection_b200")
+    if pkg not in sys.path:
+        sys.path.insert(0, pkg)
+    import train_floor_proposer as tfp
 
     net = FloorProposerNet.load(DEFAULT_WEIGHTS, max_batch=4)
     zero = _constant_proposer(cuda, 0)
-    dims = MASKS["dims"]
-    probs = np.linspace(0.5, 0.8, 16)
-    states = _states(dims, range(900, 916), probs, radius=1.0) + _states(dims, range(920, 924), (0.3, 0.45, 0.55, 0.6))
-    plain, rule = _policies(cuda, dims, zero)
-    _, learned = _policies(cuda, dims, net)
+    states = tfp.make_states(512, seed=1)[:128]
+    stack = dict(PLAIN_JACOBI_STACK, fine_smoother="fp32")
     tot = {"plain": [0, 0, 0], "rule": [0, 0, 0], "learned": [0, 0, 0]}
-    for d in states:
-        dd = cuda.as_tensor(d, device="cuda")
-        rp, rr, rl = plain.run(dd), rule.run(dd), learned.run(dd)
-        for k, r in (("plain", rp), ("rule", rr), ("learned", rl)):
-            tot[k][0] += r["total_iters"]
-            tot[k][1] += r["solve_converged"]
-            tot[k][2] += int(r["recommended_rho_min"] == rp["recommended_rho_min"])
+    for dims in tfp.MESHES:
+        spec = cantilever_spec(*dims)
+        pols = {"plain": GuardedFloorPolicy(spec, stack=stack, **tfp.POLICY),
+                "rule": LearnedFloorPolicy(spec, proposer=zero, dims=dims, stack=stack, **tfp.POLICY),
+                "learned": LearnedFloorPolicy(spec, proposer=net, dims=dims, stack=stack, **tfp.POLICY)}
+        for st in states:
+            if st["dims"] != dims:
+                continue
+            dd = cuda.as_tensor(st["density"], device="cuda")
+            rows = {k: p.run(dd) for k, p in pols.items()}
+            for k, r in rows.items():
+                tot[k][0] += r["total_iters"]
+                tot[k][1] += r["solve_converged"]
+                tot[k][2] += int(r["recommended_rho_min"] == rows["plain"]["recommended_rho_min"])
     print("outer iterations / guarded / same floor as plain:", tot)
     assert tot["learned"][1] >= tot["plain"][1]
     assert tot["learned"][0] < tot["plain"][0]
-    assert tot["learned"][2] >= 0.8 * len(states)
+    assert tot["learned"][0] <= 1.02 * tot["rule"][0]
+    assert tot["learned"][2] >= 0.95 * len(states)

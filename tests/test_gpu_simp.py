@@ -111,3 +111,48 @@ def test_short_loop_is_guarded_and_descends(cuda, policy):
     assert all(r["true_rel_residual"] <= 1e-6 for r in rows)
     assert all(abs(r["volume"] - 0.3) < 1e-3 for r in rows[1:])
     assert rows[-1]["compliance"] < rows[0]["compliance"]
+
+
+@pytest.mark.parametrize("case", [0, 1, 2, 3])
+def test_projected_oc_update_matches_reference_outputs(cuda, case):
+    """With the Heaviside projection (beta 1, 4, 16, 32; the reference's default
+    loop projects): the device projection and its derivative against the
+    reference's _heaviside / _heaviside_deriv (1e-14 / 1e-13 relative), and the
+    device OC step against the reference's own _oc_step_cupy with use_heaviside
+    (new densities to 1e-8, the last bisection bracket; the same change)."""
+    import os
+
+    from gpu_fem.simp_loop import OCUpdater, cone_filter, heaviside
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "oc_reference.npz"))
+    rmin, volfrac, move, beta, eta = (float(v) for v in g[f"h{case}/params"])
+    dims = (24, 12, 6)
+    rho = cuda.as_tensor(g[f"h{case}/rho"], device="cuda")
+    rho_f = cone_filter(rho, dims, rmin)
+    p = heaviside(rho_f, beta, eta).cpu().numpy()
+    dp = heaviside(rho_f, beta, eta, derivative=True).cpu().numpy()
+    assert np.abs(p - g[f"h{case}/proj"]).max() <= 1e-14
+    assert np.abs(dp - g[f"h{case}/dproj"]).max() <= 1e-13 * np.abs(g[f"h{case}/dproj"]).max()
+    dc = cuda.as_tensor(g[f"h{case}/dc_phys"], device="cuda")
+    rn, change, lm, steps = OCUpdater().projected(dims, rmin, rho, rho_f, dc, beta, eta, volfrac, move)
+    np.testing.assert_allclose(rn.cpu().numpy(), g[f"h{case}/rn"], rtol=0, atol=1e-8)
+    assert change == pytest.approx(float(g[f"h{case}/change"][0]), abs=1e-8)
+    # and against the oracle's restatement: the same bisection
+    H = osol.density_filter(*dims, rmin)
+    rn_o, _, lm_o, steps_o = osimp.oc_update_projected(g[f"h{case}/rho"], H @ g[f"h{case}/rho"],
+                                                       g[f"h{case}/dc_phys"], H, volfrac, move, beta, eta)
+    assert steps == steps_o and abs(lm - lm_o) <= 1e-9
+
+
+def test_projected_loop_doubles_beta_and_stays_guarded(cuda):
+    """A 22-iteration loop with the projection: beta 1 through iteration 20, 2
+    after it (the reference's continuation), every solve guarded, the projected
+    volume at the target within the bisection's resolution."""
+    from gpu_fem.simp_loop import run_simp_guarded
+
+    res = run_simp_guarded((24, 12, 6), max_iter=22, policy="plain", restart=100, seed=0, use_heaviside=True)
+    rows = res["iterations"]
+    assert res["all_guarded"] and all(r["true_rel_residual"] <= 1e-6 for r in rows)
+    assert [r["beta"] for r in rows] == [1.0] * 20 + [2.0] * 2
+    assert all(abs(r["volume"] - 0.3) < 2e-3 for r in rows[1:])
+    assert rows[-1]["compliance"] < rows[0]["compliance"]

@@ -136,6 +136,20 @@ __device__ __forceinline__ void elem_bf16(const float (&u)[8][3], float E, float
 // times).  Thread t loads the values t, t + NT, ... of the flattened tile; the
 // offsets do not depend on the plane and are computed once.
 constexpr int kTileLoads = 6;  // enough for every shape with bj >= 2, bk >= 3; launch checks
+constexpr int kPlaneBufs = 4;  // node-plane tiles: two being read, two in flight
+
+// One element copied global -> shared asynchronously (cp.async; zero-filled when
+// ok is false, reading nothing from src, which is then any valid address).
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst, const T* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 4 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 template <typename T, int EPI, int KMODE, int MAXT>
 __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh, const T* __restrict__ E,
@@ -147,7 +161,7 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
   const int W = 3 * (sh.bk + 1);   // values per tile row
   const int PV = (sh.bj + 1) * W;  // values per plane tile
   T* F = reinterpret_cast<T*>(smem_raw);  // face sums [2][12][NT]
-  T* P = F + 24 * NT;                     // node-plane tiles [3][PV]
+  T* P = F + 24 * NT;                     // node-plane tiles [kPlaneBufs][PV]
   const int t = threadIdx.x;
   const int tj = t / sh.bk, tk = t - tj * sh.bk;
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);  // ceil((nz+1)/(bk-1))
@@ -172,20 +186,21 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
     okq[q] = v < PV && j >= 0 && j <= g.ny && k >= 0 && k <= g.nz;
     rel[q] = okq[q] ? (int)(3 * ((int64_t)j * NZ1 + kb) + col) : 0;
   }
-  auto load_plane = [&](int p, T (&r)[kTileLoads]) {
+  // node plane p (zeros outside the mesh) into tile buffer p mod kPlaneBufs,
+  // asynchronously; every call commits one copy group
+  auto issue_plane = [&](int p) {
     const bool pv = p >= 0 && p <= g.nx;
     const int64_t base = pv ? (int64_t)p * plane_vals : 0;
-#pragma unroll
-    for (int q = 0; q < kTileLoads; ++q)
-      if (q * NT < PV) r[q] = (pv && okq[q]) ? u[base + rel[q]] : T(0);
-  };
-  auto store_plane = [&](int buf, const T (&r)[kTileLoads]) {
-    T* dst = P + buf * PV;
+    T* dst = P + (p & (kPlaneBufs - 1)) * PV;
 #pragma unroll
     for (int q = 0; q < kTileLoads; ++q) {
       const int v = t + q * NT;
-      if (q * NT < PV && v < PV) dst[v] = r[q];
+      if (q * NT < PV && v < PV) {
+        const bool ok = pv && okq[q];
+        cp_async_elem(dst + v, ok ? u + base + rel[q] : u, ok);
+      }
     }
+    cp_async_commit();
   };
   auto read_face = [&](int buf, T (&uu)[4][3]) {
     const T* src = P + buf * PV;
@@ -198,13 +213,12 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
   };
   auto e_index = [&](int ie) { return ((int64_t)ie * g.ny + je) * g.nz + ke; };
 
-  // prologue: planes i0-1 and i0 into the tile buffers, plane i0+1 in flight
-  T pre[kTileLoads];
-  load_plane(i0 - 1, pre);
-  store_plane((i0 + 2) % 3, pre);
-  load_plane(i0, pre);
-  store_plane(i0 % 3, pre);
-  if (i0 + 1 <= i1) load_plane(i0 + 1, pre);
+  // prologue: planes i0-1 and i0 in the tile buffers, plane i0+1 in flight
+  issue_plane(i0 - 1);
+  issue_plane(i0);
+  if (i0 + 1 <= i1) issue_plane(i0 + 1);
+  else cp_async_commit();
+  cp_async_wait_all_but_one();
   T Enext = (colv && i0 - 1 >= 0 && i0 - 1 < g.nx) ? E[e_index(i0 - 1)] : T(0);
   T carry[4][3];
 #pragma unroll
@@ -214,13 +228,14 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
   __syncthreads();
 
   // Element plane ie couples node planes ie and ie + 1, both read from the
-  // three rotating tile buffers (plane q in buffer q mod 3).  One barrier per
-  // plane: the tile of plane ie + 2 is written before it and first read after
-  // it, the buffer it overwrites (plane ie - 1) was last read before the
-  // previous barrier, and the face sums alternate between two buffers.
+  // rotating tile buffers (plane q in buffer q mod 4).  One barrier per plane:
+  // the copy of plane ie + 3 is issued at the top (its buffer held plane ie - 1,
+  // last read before the previous barrier), and before the barrier every thread
+  // waits for its copies of plane ie + 2, so after it the next iteration's two
+  // planes are complete and visible; the face sums alternate between two buffers.
   for (int ie = i0 - 1; ie < i1; ++ie) {
-    if (ie + 2 <= i1) store_plane((ie + 2) % 3, pre);
-    if (ie + 3 <= i1) load_plane(ie + 3, pre);
+    if (ie + 3 <= i1) issue_plane(ie + 3);
+    else cp_async_commit();
     const T Ee = Enext;
     Enext = (colv && ie + 1 < g.nx) ? E[e_index(ie + 1)] : T(0);
     const bool do_epi = own && ie >= i0;
@@ -228,7 +243,7 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
     if (do_epi) node = ((int64_t)ie * (g.ny + 1) + je) * NZ1 + ke;
     EpiOperands<T, EPI> eo;
     if (do_epi) eo.load(ea, 3 * node, mask);
-    const int blo = (ie + 3) % 3, bhi = (ie + 1) % 3;
+    const int blo = ie & (kPlaneBufs - 1), bhi = (ie + 1) & (kPlaneBufs - 1);
     // the node's own value, read before the barrier: after it the next
     // iteration may overwrite this plane's buffer
     T xv[3];
@@ -260,6 +275,7 @@ __global__ void __launch_bounds__(MAXT) fine_sweep_kernel(Grid g, SweepShape sh,
 #pragma unroll
         for (int c = 0; c < 3; ++c) buf[(q2 * 3 + c) * NT + t] = carry[q2][c] + f[q2][c];
     }
+    cp_async_wait_all_but_one();
     __syncthreads();
     if (do_epi) {
 #pragma unroll
@@ -281,7 +297,7 @@ template <typename T>
 static size_t sweep_smem(const SweepShape& sh) {
   const size_t NT = (size_t)sh.bj * sh.bk;
   const size_t PV = (size_t)(sh.bj + 1) * 3 * (sh.bk + 1);
-  return (24 * NT + 3 * PV) * sizeof(T);
+  return (24 * NT + kPlaneBufs * PV) * sizeof(T);
 }
 
 template <typename T, int EPI, int KMODE, int MAXT>
@@ -364,8 +380,8 @@ __device__ __forceinline__ void elem_wht_x2(const float2 (&u)[8][3], float2 E, f
 constexpr int kX2Threads = 256;
 constexpr int kX2NodeLoads = 3;  // tile nodes per thread; launch checks
 
-template <int EPI>
-__global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, SweepShape sh,
+template <int EPI, int MINB>
+__global__ void __launch_bounds__(kX2Threads, MINB) fine_sweep_x2_kernel(Grid g, SweepShape sh,
                                                                    const float* __restrict__ E,
                                                                    const uint8_t* __restrict__ mask,
                                                                    const float* __restrict__ u, EpiArgs ea) {
@@ -404,6 +420,8 @@ __global__ void __launch_bounds__(kX2Threads) fine_sweep_x2_kernel(Grid g, Sweep
     rel[s] = okn[s] ? 3 * (j * NZ1 + k) : 0;
     sidx[s] = n < NN ? row * NKP + kk : -1;
   }
+  // (the packed sweep stages its planes through registers: with cp.async it
+  // needed 214 registers for the Jacobi epilogue and ran slower)
   auto load_plane = [&](int p, float (&r)[3 * kX2NodeLoads]) {
     const bool pv = p >= 0 && p <= g.nx;
     const float* base = u + (pv ? (int64_t)p * plane_vals : 0);
@@ -517,18 +535,25 @@ static bool x2_shape_ok(const Grid& g, const SweepShape& sh) {
 template <int EPI>
 static cudaError_t launch_sweep_f32(const Grid& g, const SweepShape& sh, const float* E, const uint8_t* mask,
                                     const float* u, const EpiArgs& ea, cudaStream_t s) {
-  if (sh.one || !x2_shape_ok(g, sh)) return launch_sweep<float, EPI, 0, 512>(g, sh, E, mask, u, ea, s);
+  if (sh.variant == 1 || !x2_shape_ok(g, sh)) return launch_sweep<float, EPI, 0, 512>(g, sh, E, mask, u, ea, s);
   const int NT = sh.bj * sh.bk / 2, NE = sh.bj * sh.bk;
   const size_t smem = sizeof(float) * (36 * (size_t)NE + 9 * (size_t)(sh.bj + 1) * (sh.bk + 2));
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = true;
+  static bool attr_done[2] = {false, false};
+  const int capped = sh.variant == 2 ? 1 : 0;
+  if (!attr_done[capped]) {
+    if (capped)
+      cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    else
+      cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done[capped] = true;
   }
   const int nbj = (g.ny + sh.bj - 1) / (sh.bj - 1);
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
   dim3 grid(nbj * nbk, div_up(g.nx + 1, sh.cx));
-  fine_sweep_x2_kernel<EPI><<<grid, NT, smem, s>>>(g, sh, E, mask, u, ea);
+  if (capped)
+    fine_sweep_x2_kernel<EPI, 2><<<grid, NT, smem, s>>>(g, sh, E, mask, u, ea);
+  else
+    fine_sweep_x2_kernel<EPI, 1><<<grid, NT, smem, s>>>(g, sh, E, mask, u, ea);
   return sf_launched(1);
 }
 

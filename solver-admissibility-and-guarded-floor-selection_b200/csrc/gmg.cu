@@ -228,12 +228,15 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
         sh.bk = bk;
         sh.cx = cx;
         cands.push_back(sh);
-        // FP32: the one-element-per-thread sweep as well; it has twice the threads
-        // of the packed sweep for the same tile, which can hide more latency on grids
-        // too small to fill the GPU with packed blocks
+        // FP32: also the one-element-per-thread sweep (twice the threads of the packed
+        // sweep for the same tile) and the packed sweep with a register cap (more
+        // resident blocks); on grids too small to fill the GPU either can hide more
+        // latency than the packed sweep
         if (t == F32) {
-          sh.one = 1;
-          cands.push_back(sh);
+          for (int v : {1, 2}) {
+            sh.variant = v;
+            cands.push_back(sh);
+          }
         }
       }
     }
@@ -261,8 +264,8 @@ void tune_mesh(Mesh& m, DType t, cudaStream_t s) {
     float ms = 0.f;
     SF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     if (verbose)
-      fprintf(stderr, "[simpfem tune] %s %dx%dx%d bj=%d bk=%d cx=%d one=%d: %.1f us\n", t == F64 ? "f64" : "f32",
-              m.g.nx, m.g.ny, m.g.nz, sh.bj, sh.bk, sh.cx, sh.one, ms * 1000.f / 3.f);
+      fprintf(stderr, "[simpfem tune] %s %dx%dx%d bj=%d bk=%d cx=%d variant=%d: %.1f us\n",
+              t == F64 ? "f64" : "f32", m.g.nx, m.g.ny, m.g.nz, sh.bj, sh.bk, sh.cx, sh.variant, ms * 1000.f / 3.f);
     if (ms < best) {
       best = ms;
       best_sh = sh;

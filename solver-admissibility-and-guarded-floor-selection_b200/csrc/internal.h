@@ -60,8 +60,9 @@ struct SweepShape {
   int bj = 8;   // element columns along y per block (one of them is a halo column)
   int bk = 32;  // element columns along z per block (one halo column)
   int cx = 8;   // node planes along x per block
-  int one = 0;  // FP32: 1 = one element per thread (the scalar sweep) even where the
-                // two-element packed sweep applies; picked by the tuner like the tile
+  int variant = 0;  // FP32 kernel, picked by the tuner like the tile: 0 = two elements per
+                    // thread (packed FP32 pairs), 1 = one element per thread, 2 = two per
+                    // thread compiled for two resident 256-thread blocks (a 128-register cap)
 };
 
 struct WhtBlocks {

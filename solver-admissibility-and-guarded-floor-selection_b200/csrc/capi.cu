@@ -524,9 +524,10 @@ int simpfem_dense_cholesky_inverse(int n, double* A, double* Linv, int* info_hos
   SF_API_BEGIN
   if (n < 0 || (n > 0 && (!A || !Linv)) || !info_host)
     throw InvalidArg{"simpfem_dense_cholesky_inverse: bad argument"};
-  DevBuf info;
+  DevBuf info, dinv;
   info.alloc(2 * sizeof(int));
-  SF_CUDA(dense_chol_inverse(A, n, Linv, info.as<int>(), S(stream)));
+  dinv.alloc(band_dinv_bytes(n));
+  SF_CUDA(dense_chol_inverse(A, n, Linv, dinv.as<double>(), info.as<int>(), S(stream)));
   SF_CUDA(cudaMemcpyAsync(info_host, info.p, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
   SF_CUDA(cudaStreamSynchronize(S(stream)));
   SF_API_END

@@ -1,4 +1,6 @@
-// Dense FP64 factorisation of the coarsest-level matrix.
+// Dense FP64 factorisation of the coarsest-level matrix: the entry
+// (chol_inverse), and the recursion that takes matrices whose band is too wide
+// for the band path in bandchol.cu.
 //
 // The reference factors the assembled coarsest matrix with cp.linalg.cholesky,
 // treats a failed factorisation (info != 0 or a non-finite factor) as the
@@ -327,7 +329,8 @@ __global__ void lower_band_kernel(const double* __restrict__ A, int n, int* __re
   if (lane == 0 && i - first > 0) atomicMax(bw, i - first);
 }
 
-__global__ void transpose_kernel(const double* __restrict__ A, int n, double* __restrict__ At) {
+template <typename OT>
+__global__ void transpose_kernel(const double* __restrict__ A, int n, OT* __restrict__ At) {
   __shared__ double T[32][33];
   const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
@@ -337,7 +340,7 @@ __global__ void transpose_kernel(const double* __restrict__ A, int n, double* __
   __syncthreads();
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int i = bx + r, j = by + threadIdx.x;
-    if (i < n && j < n) At[(int64_t)i * n + j] = T[threadIdx.x][r];
+    if (i < n && j < n) At[(int64_t)i * n + j] = (OT)T[threadIdx.x][r];
   }
 }
 
@@ -349,17 +352,21 @@ __global__ void nonfinite_flag_kernel(const double* __restrict__ A, int64_t n, i
     }
 }
 
+template <typename OT>
+cudaError_t launch_transpose(const double* A, int n, OT* At, cudaStream_t s) {
+  const int nb = div_up(n, 32);
+  transpose_kernel<OT><<<dim3(nb, nb), dim3(32, 8), 0, s>>>(A, n, At);
+  return sf_launched(1);
+}
+
 }  // namespace
 
-cudaError_t dense_chol_inverse(double* A, int n, double* Linv, int* info_dev, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(info_dev, 0, sizeof(int), s);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, s);
+cudaError_t chol_inverse(double* A, int n, double* work64, double* dinv, const BandInvOut& out, int* info_dev,
+                         cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(info_dev, 0, 2 * sizeof(int), s);
   if (e != cudaSuccess) return e;
   if (n <= 0) return cudaSuccess;
-  // the band (exact zeros below it) decides which blocks the recursion multiplies
-  e = cudaMemsetAsync(info_dev + 1, 0, sizeof(int), s);
-  if (e != cudaSuccess) return e;
+  // the band (exact zeros below it) decides the path and the blocks multiplied
   lower_band_kernel<<<div_up((int64_t)n * 32, 256), 256, 0, s>>>(A, n, info_dev + 1);
   e = sf_launched(1);
   if (e != cudaSuccess) return e;
@@ -368,18 +375,35 @@ cudaError_t dense_chol_inverse(double* A, int n, double* Linv, int* info_dev, cu
   if (e != cudaSuccess) return e;
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
-  e = chol_inv_rec(A, Linv, n, 0, n, std::max(bw, 0), info_dev, s);
-  if (e != cudaSuccess) return e;
+  bw = std::max(bw, 0);
+  if (band_tiles(bw) <= kBandMaxTiles) return band_chol_inverse(A, n, bw, dinv, out, info_dev, s);
   const int64_t nn = (int64_t)n * n;
-  nonfinite_flag_kernel<<<(int)std::min<int64_t>(div_up(nn, 256), 148 * 16), 256, 0, s>>>(Linv, nn, n + 1,
+  e = cudaMemsetAsync(work64, 0, sizeof(double) * (size_t)nn, s);
+  if (e != cudaSuccess) return e;
+  e = chol_inv_rec(A, work64, n, 0, n, bw, info_dev, s);
+  if (e != cudaSuccess) return e;
+  nonfinite_flag_kernel<<<(int)std::min<int64_t>(div_up(nn, 256), 148 * 16), 256, 0, s>>>(work64, nn, n + 1,
                                                                                           info_dev);
-  return sf_launched(1);
+  e = sf_launched(1);
+  if (e != cudaSuccess) return e;
+  if (out.L64 && out.L64 != work64) {
+    e = cudaMemcpyAsync(out.L64, work64, sizeof(double) * (size_t)nn, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
+  }
+  if (out.LT64 && (e = launch_transpose(work64, n, out.LT64, s)) != cudaSuccess) return e;
+  if (out.L32 && (e = launch_convert(F64, F32, work64, out.L32, nn, nullptr, s)) != cudaSuccess) return e;
+  if (out.LT32 && (e = launch_transpose(work64, n, out.LT32, s)) != cudaSuccess) return e;
+  return cudaSuccess;
 }
 
-cudaError_t launch_transpose(const double* A, int n, double* At, cudaStream_t s) {
-  const int nb = div_up(n, 32);
-  transpose_kernel<<<dim3(nb, nb), dim3(32, 8), 0, s>>>(A, n, At);
-  return sf_launched(1);
+cudaError_t dense_chol_inverse(double* A, int n, double* Linv, double* dinv, int* info_dev, cudaStream_t s) {
+  if (n > 0) {
+    const cudaError_t e = cudaMemsetAsync(Linv, 0, sizeof(double) * (size_t)n * n, s);
+    if (e != cudaSuccess) return e;
+  }
+  BandInvOut out;
+  out.L64 = Linv;
+  return chol_inverse(A, n, Linv, dinv, out, info_dev, s);
 }
 
 }  // namespace simpfem

@@ -1144,14 +1144,28 @@ static void setup_coarsest(Gmg& G) {
   G.coarse_reg = false;
   const int n = G.nc;
   if (n <= G.o.dense_chol_max && n > 0) {
-    G.Adense.alloc(8 * (size_t)n * n);
-    G.Linv.alloc(8 * (size_t)n * n);
+    const size_t nn = (size_t)n * n;
+    G.Adense.alloc(8 * nn);
+    G.Linv.alloc(8 * nn);  // the FP64 cycle's L^{-1}; the wide-band recursion's work array
+    G.cdinv.alloc(band_dinv_bytes(n));
+    BandInvOut out;
+    if (G.cyc == F32) {
+      // the mixed cycle reads FP32 copies of both factors (FP64 accumulation)
+      G.LinvF.alloc(4 * nn);
+      G.LinvTF.alloc(4 * nn);
+      out.L32 = G.LinvF.as<float>();
+      out.LT32 = G.LinvTF.as<float>();
+    } else {
+      G.LinvT.alloc(8 * nn);
+      out.L64 = G.Linv.as<double>();
+      out.LT64 = G.LinvT.as<double>();
+    }
     int* info = G.cinfo.as<int>();
     auto try_factor = [&](double eps) -> bool {
       SF_CUDA(launch_stencil_to_dense(L.g, L.K64.as<double>(), G.c_didx.as<int32_t>(), n, G.Adense.as<double>(),
                                       G.st));
       if (eps > 0) SF_CUDA(launch_add_diag(G.Adense.as<double>(), n, eps, G.st));
-      SF_CUDA(dense_chol_inverse(G.Adense.as<double>(), n, G.Linv.as<double>(), info, G.st));
+      SF_CUDA(chol_inverse(G.Adense.as<double>(), n, G.Linv.as<double>(), G.cdinv.as<double>(), out, info, G.st));
       int h = 0;
       SF_CUDA(cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, G.st));
       SF_CUDA(cudaStreamSynchronize(G.st));
@@ -1175,16 +1189,6 @@ static void setup_coarsest(Gmg& G) {
       }
     }
     if (ok) {
-      G.LinvT.alloc(8 * (size_t)n * n);
-      SF_CUDA(launch_transpose(G.Linv.as<double>(), n, G.LinvT.as<double>(), G.st));
-      if (G.cyc == F32) {
-        // the mixed cycle reads FP32 copies of both factors (FP64 accumulation)
-        const int64_t nn2 = (int64_t)n * n;
-        G.LinvF.alloc(4 * (size_t)nn2);
-        G.LinvTF.alloc(4 * (size_t)nn2);
-        SF_CUDA(launch_convert(F64, F32, G.Linv.p, G.LinvF.p, nn2, nullptr, G.st));
-        SF_CUDA(launch_convert(F64, F32, G.LinvT.p, G.LinvTF.p, nn2, nullptr, G.st));
-      }
       G.coarse_mode = 1;
       return;
     }

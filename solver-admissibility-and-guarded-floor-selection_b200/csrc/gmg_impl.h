@@ -193,6 +193,7 @@ struct Gmg {
   int nc = 0;
   DevBuf c_idx, c_didx, Adense, Linv, LinvT, cb, cx, ctmp, cinfo;
   DevBuf LinvF, LinvTF;  // FP32 copies of Linv and LinvT read by the mixed cycle
+  DevBuf cdinv;          // inverses of the diagonal tiles of the coarsest factor (scratch)
   // iterative coarse (fixed PCG) vectors
   DevBuf pr, pz, pp, pAp;
 

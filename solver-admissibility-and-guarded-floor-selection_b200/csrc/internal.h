@@ -189,13 +189,33 @@ cudaError_t launch_enrich_rhs(int64_t n, int mode, const double* w, double wfloo
                               const double* p, const uint8_t* mask, double* out, const int* guard,
                               cudaStream_t s);
 
-// Linv <- L^{-1} (lower, zero upper) of the Cholesky factor of the SPD row-major
-// A (destroyed).  info_dev[0]: 0, or the 1-based index of the first non-positive
-// pivot, or n + 1 when L^{-1} holds a non-finite entry; info_dev[1] is scratch
-// (the measured lower bandwidth of A, which decides the blocks multiplied).
-// Synchronises the stream once (the bandwidth is read on the host).
-cudaError_t dense_chol_inverse(double* A, int n, double* Linv, int* info_dev, cudaStream_t s);
-cudaError_t launch_transpose(const double* A, int n, double* At, cudaStream_t s);
+// Outputs of the factorisation: any of L^{-1} and L^{-T}, row-major n x n, in
+// FP64 or FP32 (null: not written).  Entries on and below (L^{-1}) or on and
+// above (L^{-T}) the diagonal are written; the other triangle is left as it is.
+struct BandInvOut {
+  double* L64 = nullptr;
+  double* LT64 = nullptr;
+  float* L32 = nullptr;
+  float* LT32 = nullptr;
+};
+// The band path (bandchol.cu) takes matrices with ceil(bw / 32) <= kBandMaxTiles.
+constexpr int kBandMaxTiles = 24;
+int band_tiles(int bw);
+size_t band_dinv_bytes(int n);  // scratch of the band path: the inverses of L's diagonal tiles
+cudaError_t band_chol_inverse(double* A, int n, int bw, double* dinv, const BandInvOut& out, int* info,
+                              cudaStream_t s);
+// L^{-1} of the Cholesky factor of the SPD row-major A (destroyed) into the
+// requested outputs.  The lower bandwidth bw of A is measured (one stream
+// synchronisation); with ceil(bw / 32) <= kBandMaxTiles the band path writes
+// the outputs directly, else the recursion in dense.cu factors into work64
+// (n x n FP64) and the outputs are copied / transposed / converted from it.
+// info_dev[0]: 0, or the 1-based index of the first non-positive pivot, or
+// n + 1 when L^{-1} holds a non-finite entry; info_dev[1] is scratch.  dinv:
+// band_dinv_bytes(n) of scratch.
+cudaError_t chol_inverse(double* A, int n, double* work64, double* dinv, const BandInvOut& out, int* info_dev,
+                         cudaStream_t s);
+// Linv <- L^{-1} (lower, zero upper): chol_inverse into a zeroed Linv.
+cudaError_t dense_chol_inverse(double* A, int n, double* Linv, double* dinv, int* info_dev, cudaStream_t s);
 cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b,
                                   double* tmp, double* x, const int* guard, cudaStream_t s);
 // the same with FP32 copies of L^{-1} and L^{-T} (FP64 vectors and accumulation)

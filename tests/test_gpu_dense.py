@@ -112,3 +112,31 @@ def test_banded_with_one_wide_row_and_scales(cuda):
     assert info == 0
     x = Li.T @ (Li @ b)
     assert np.linalg.norm(A @ x - b) <= 1e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("n,bw", [(600, 300), (1000, 219), (1600, 760)])
+def test_band_path_repeatable(cuda, n, bw):
+    """The band path (one thread-block cluster exchanging tiles through shared
+    memory and L2) gives the same bits on every run, at band widths below, at and
+    beyond the cluster's eight tile rows, up to its widest band (24 tiles)."""
+    A = _banded_spd(n, bw, 11 * n + bw)
+    ref = np.linalg.inv(np.linalg.cholesky(A))
+    first = None
+    for _ in range(8):
+        Li, info = _factor(cuda, A)
+        assert info == 0
+        assert np.abs(Li - ref).max() <= 1e-12 * np.abs(ref).max()
+        if first is None:
+            first = Li
+        else:
+            assert np.array_equal(Li, first)
+
+
+def test_wide_band_takes_the_recursion(cuda):
+    # 26 tiles below the diagonal: beyond the band path, the recursion factors it
+    n, bw = 1200, 820
+    A = _banded_spd(n, bw, 3)
+    Li, info = _factor(cuda, A)
+    ref = np.linalg.inv(np.linalg.cholesky(A))
+    assert info == 0
+    assert np.abs(Li - ref).max() <= 1e-12 * np.abs(ref).max()

@@ -12,13 +12,13 @@
 //
 // 1. band_chol_kernel: one thread-block cluster (8 CTAs, distributed shared
 //    memory) runs the tiled right-looking band Cholesky over 32 x 32 tiles,
-//    with WB = ceil(bw / 32) tiles below the diagonal.  Step K: the CTAs owning
-//    tile rows K+1..K+WB form L_IK = A_IK L_KK^{-T} on the FP64 tensor cores
-//    (mma.sync m8n8k4), L_KK^{-1} copied from the distributed shared memory of
-//    the CTA that made it; the CTA owning row K+1 then subtracts
+//    with WB = ceil(bw / 32) tiles below the diagonal.  CTA 0 makes every
+//    diagonal factor: step K, it forms L_{K+1,K} = A_{K+1,K} L_KK^{-T} on the
+//    FP64 tensor cores (mma.sync m8n8k4) with its own L_KK^{-1}, subtracts
 //    L_{K+1,K} L_{K+1,K}^T from A_{K+1,K+1}, factors it and inverts the factor
-//    (one warp, pivot column broadcast through shared memory), while the warps
-//    of the other CTAs apply the rest of the trailing update
+//    (one warp, pivot column broadcast through shared memory).  The seven other
+//    CTAs copy L_KK^{-1} from CTA 0's distributed shared memory, form L_IK for
+//    I = K+2..K+WB the same way and apply the rest of the trailing update
 //    A_IJ -= L_IK L_JK^T, half a tile per warp on the tensor cores with
 //    fragments loaded from L2.  Two cluster barriers a step.  The inverses of
 //    the diagonal tiles are kept for step 2.
@@ -85,13 +85,13 @@ __device__ __forceinline__ void store_tile(double* __restrict__ A, int n, int I,
 }
 
 // Warp 0: Cholesky of the 32 x 32 tile in T and the inverse of the factor,
-// pivot K.  Lane i holds row i of the tile in a register window shifted one
-// column per pivot (w[c] = column j + c at pivot j), so the loop body does not
-// change with j and stays a short loop: this code runs once every CL steps of
-// the cluster and would otherwise be fetched cold each time.  Lane c also
-// holds column c of L^{-1} (x[c'] = row j + c' at pivot j), formed
-// right-looking from the same broadcast pivot column.  Outputs: the factor in
-// T (lower, zero upper), L^{-1} row-major in D (stride T36).
+// pivot K, fully unrolled so that every register index is a constant.  Lane i
+// holds row i of the tile (w) and column i of L^{-1} (x, formed right-looking
+// from the same broadcast pivot column).  Only lane j+1's own update of its
+// diagonal entry sits on the chain between two pivots; the other columns'
+// updates fill the issue slots.  The dedicated factor CTA runs this every step,
+// so its ~1,700 instructions stay in that SM's instruction cache.  Outputs: the
+// factor in T (lower, zero upper), L^{-1} row-major in D (stride T36).
 __device__ void potrf_inv_tile(double* T, double* col, double* D, int K, int n, int* info) {
   const int lane = threadIdx.x & 31, o = TS * K;
   double w[32], x[32];
@@ -100,29 +100,36 @@ __device__ void potrf_inv_tile(double* T, double* col, double* D, int K, int n, 
     w[c] = T[lane * T33 + c];
     x[c] = c == lane ? 1.0 : 0.0;
   }
-  col[32 + lane] = 0.0;  // col[32..63] and col[96..127] stay zero: reads past column 31
-  col[96 + lane] = 0.0;
-#pragma unroll 1
+#pragma unroll
   for (int j = 0; j < 32; ++j) {
-    double d = __shfl_sync(FULL, w[0], j);
+    double d = __shfl_sync(FULL, w[j], j);
     if (!(d > 0.0) || !isfinite(d)) {
       d = 1.0;
       if (lane == 0 && o + j < n) atomicCAS(info, 0, o + j + 1);
     }
     const double rs = rsqrt(d);
-    const double l = lane > j ? w[0] * rs : (lane == j ? d * rs : 0.0);  // column j of L
+    const double l = lane > j ? w[j] * rs : (lane == j ? d * rs : 0.0);  // column j of L
     T[lane * T33 + j] = l;
-    double* cb = col + (j & 1) * 64;  // two buffers: one __syncwarp a pivot
+    double* cb = col + (j & 1) * 32;  // two buffers: one __syncwarp a pivot
     cb[lane] = lane > j ? l : 0.0;
     __syncwarp();
     const double lm = lane > j ? l : 0.0;
-    const double xj = x[0] * rs;  // row j of L^{-1}: (row j so far) / L_jj
+    const double xj = x[j] * rs;  // row j of L^{-1}: (row j so far) / L_jj
     D[j * T36 + lane] = xj;
+    int cs = j + 1;
+    if ((cs & 1) && cs < 32) {
+      const double lc = cb[cs];
+      w[cs] = fma(-lm, lc, w[cs]);
+      x[cs] = fma(-xj, lc, x[cs]);
+      ++cs;
+    }
 #pragma unroll
-    for (int c = 1; c < 32; ++c) {
-      const double lc = cb[j + c];
-      w[c - 1] = fma(-lm, lc, w[c]);
-      x[c - 1] = fma(-xj, lc, x[c]);
+    for (int c = cs; c < 32; c += 2) {
+      const double2 v = *reinterpret_cast<const double2*>(cb + c);
+      w[c] = fma(-lm, v.x, w[c]);
+      x[c] = fma(-xj, v.x, x[c]);
+      w[c + 1] = fma(-lm, v.y, w[c + 1]);
+      x[c + 1] = fma(-xj, v.y, x[c + 1]);
     }
   }
 }
@@ -238,20 +245,19 @@ __device__ void update_half_tile(double* __restrict__ A, int n, int I, int J, in
 
 // Shared memory of one factorisation CTA (doubles).
 struct CholSmem {
-  static constexpr int D = 0;                // [32][T36] this CTA's last L_KK^{-1} (read by the cluster)
-  static constexpr int DL = D + 32 * T36;    // [32][T36] local copy of the step's L_KK^{-1}
-  static constexpr int TQ = DL + 32 * T36;   // [32][T33] L_{K+1,K} of the next pivot's CTA
-  static constexpr int TP = TQ + 32 * T33;   // [32][T33] A_{K+1,K+1}, then its factor
-  static constexpr int COL = TP + 32 * T33;  // [2][64] pivot column (upper halves zero)
-  static constexpr int TOTAL = COL + 128;
+  static constexpr int D = 0;                 // [2][32][T36] the factor CTA's L_KK^{-1}, by K % 2
+  static constexpr int DL = D + 2 * 32 * T36; // [32][T36] a worker's copy of the step's L_KK^{-1}
+  static constexpr int TQ = DL + 32 * T36;    // [32][T33] L_{K+1,K} (factor CTA)
+  static constexpr int TP = TQ + 32 * T33;    // [32][T33] A_{K+1,K+1}, then its factor (factor CTA)
+  static constexpr int COL = TP + 32 * T33;   // [2][32] pivot column
+  static constexpr int TOTAL = COL + 64;
 };
 
 // Warp 0 factors the updated diagonal tile in Tp and inverts the factor into
 // D; then the CTA stores both.
-__device__ void factor_diag(double* sm, double* __restrict__ A, int n, int K, double* __restrict__ dinv,
-                            int* info) {
+__device__ void factor_diag(double* sm, double* D, double* __restrict__ A, int n, int K,
+                            double* __restrict__ dinv, int* info) {
   double* Tp = sm + CholSmem::TP;
-  double* D = sm + CholSmem::D;
   if ((threadIdx.x >> 5) == 0) potrf_inv_tile(Tp, sm + CholSmem::COL, D, K, n, info);
   __syncthreads();
   store_tile(A, n, K, K, Tp, true);
@@ -259,76 +265,84 @@ __device__ void factor_diag(double* sm, double* __restrict__ A, int n, int K, do
   for (int e = threadIdx.x; e < 1024; e += FT) out[e] = D[(e >> 5) * T36 + (e & 31)];
 }
 
-// One cluster of CL CTAs.  WB: tiles below the diagonal in the band.  Step K:
-// the CTA of tile row I (I % CL) divides A_IK by L_KK^T for I = K+1..K+WB; the
-// CTA of row K+1 then forms and factors tile K+1 while the warps of the other
-// CTAs apply the rest of the trailing update, half a tile per warp.  Every
-// CTA runs the same sequence of cluster barriers; the branches between them
-// depend only on the step and the rank.
+// One cluster of CL CTAs: CTA 0 makes every diagonal factor, CTAs 1..CL-1 are
+// workers.  WB: tiles below the diagonal in the band.  Step K: CTA 0 divides
+// tile row K+1 by L_KK^T with its own L_KK^{-1}, then forms and factors tile
+// K+1 (its inverse into the other half of a double buffer, since the workers
+// copy the current half during the same step); the workers divide tile rows
+// K+2..K+WB (round robin) and then apply the rest of the trailing update, half
+// a tile per warp.  Every CTA runs the same sequence of cluster barriers; the
+// branches between them depend only on the step and the rank.
 __global__ void __launch_bounds__(FT) band_chol_kernel(double* __restrict__ A, int n, int NB, int WB,
                                                        double* __restrict__ dinv, int* __restrict__ info) {
   extern __shared__ __align__(16) double sm[];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int warp = threadIdx.x >> 5;
+  constexpr int NW = CL - 1;  // workers
   double* Tq = sm + CholSmem::TQ;
   double* Tp = sm + CholSmem::TP;
 
   if (rank == 0) {
     load_tile(A, n, 0, 0, Tp);
     __syncthreads();
-    factor_diag(sm, A, n, 0, dinv, info);
+    factor_diag(sm, sm + CholSmem::D, A, n, 0, dinv, info);
   }
   cluster_arrive();
   cluster_wait();
 
   for (int K = 0; K < NB; ++K) {
-    const int p = K % CL, q = (K + 1) % CL;
     const int last = min(NB - 1, K + WB);
-    const bool is_q = rank == q && K + 1 < NB;
-    const int I0 = K + 1 + ((rank - (K + 1)) % CL + CL) % CL;  // this CTA's first tile row below K
-    if (is_q) load_tile(A, n, K + 1, K + 1, Tp);
-    if (I0 <= last) {
-      // L_KK^{-1} from the distributed shared memory of the CTA that made it,
-      // copied once with all loads in flight: the step's divisions then read
-      // it locally (faster than fragment loads from the other CTA per division)
-      const double* Dp = cluster.map_shared_rank(sm + CholSmem::D, p);
-      double* Dl = sm + CholSmem::DL;
-      constexpr int NV = (32 * T36 + FT - 1) / FT;
-      double v[NV];
-#pragma unroll
-      for (int u = 0; u < NV; ++u) {
-        const int e = threadIdx.x + FT * u;
-        if (e < 32 * T36) v[u] = Dp[e];
-      }
-#pragma unroll
-      for (int u = 0; u < NV; ++u) {
-        const int e = threadIdx.x + FT * u;
-        if (e < 32 * T36) Dl[e] = v[u];
+    double* Dk = sm + CholSmem::D + (K & 1) * 32 * T36;  // L_KK^{-1} in the factor CTA's layout
+    if (rank == 0) {
+      const bool next = K + 1 < NB;
+      if (next) {
+        load_tile(A, n, K + 1, K + 1, Tp);
+        if (WB > 0) trsm_mma(A, n, K + 1, K, Dk, Tq);
       }
       __syncthreads();
-      for (int I = I0; I <= last; I += CL) trsm_mma(A, n, I, K, Dl, I == K + 1 ? Tq : nullptr);
-    }
-    __syncthreads();
-    cluster_arrive();  // the step's L_IK are in L2
-    if (is_q) {
-      if (WB > 0) {
-        syrk_smem(Tp, Tq);
-        __syncthreads();
+      cluster_arrive();  // L_{K+1,K} is in L2
+      if (next) {
+        if (WB > 0) {
+          syrk_smem(Tp, Tq);
+          __syncthreads();
+        }
+        factor_diag(sm, sm + CholSmem::D + ((K + 1) & 1) * 32 * T36, A, n, K + 1, dinv, info);
       }
-      factor_diag(sm, A, n, K + 1, dinv, info);
-    }
-    cluster_wait();
-    if (!is_q) {
-      // the rest of the trailing update in half tiles: half tile u to warp
-      // (u / (CL - 1)) % 8 of CTA (q + 1 + u % (CL - 1)) % CL
+      cluster_wait();
+    } else {
+      const int I0 = K + 1 + rank;  // this worker's first tile row
+      if (I0 <= last) {
+        // L_KK^{-1} from the factor CTA's distributed shared memory, copied once
+        // with all loads in flight: the step's divisions then read it locally
+        const double* Dp = cluster.map_shared_rank(Dk, 0);
+        double* Dl = sm + CholSmem::DL;
+        constexpr int NV = (32 * T36 + FT - 1) / FT;
+        double v[NV];
+#pragma unroll
+        for (int u = 0; u < NV; ++u) {
+          const int e = threadIdx.x + FT * u;
+          if (e < 32 * T36) v[u] = Dp[e];
+        }
+#pragma unroll
+        for (int u = 0; u < NV; ++u) {
+          const int e = threadIdx.x + FT * u;
+          if (e < 32 * T36) Dl[e] = v[u];
+        }
+        __syncthreads();
+        for (int I = I0; I <= last; I += NW) trsm_mma(A, n, I, K, Dl, nullptr);
+      }
+      __syncthreads();
+      cluster_arrive();  // the step's L_IK are in L2
+      cluster_wait();
+      // the trailing update in half tiles: half tile u to warp (u / NW) % 8 of
+      // worker 1 + u % NW
       int u = 0;
       for (int I = K + 1; I <= last; ++I)
         for (int J = K + 1; J <= I; ++J) {
           if (I == K + 1 && J == K + 1) continue;
           for (int h = 0; h < 2; ++h, ++u)
-            if ((q + 1 + u % (CL - 1)) % CL == rank && (u / (CL - 1)) % 8 == warp)
-              update_half_tile(A, n, I, J, K, h);
+            if (1 + u % NW == rank && (u / NW) % 8 == warp) update_half_tile(A, n, I, J, K, h);
         }
     }
     cluster_arrive();  // updates and the next factor are in place

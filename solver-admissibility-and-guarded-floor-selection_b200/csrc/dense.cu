@@ -362,19 +362,21 @@ cudaError_t launch_transpose(const double* A, int n, OT* At, cudaStream_t s) {
 }  // namespace
 
 cudaError_t chol_inverse(double* A, int n, double* work64, double* dinv, const BandInvOut& out, int* info_dev,
-                         cudaStream_t s) {
+                         cudaStream_t s, int bw_known) {
   cudaError_t e = cudaMemsetAsync(info_dev, 0, 2 * sizeof(int), s);
   if (e != cudaSuccess) return e;
   if (n <= 0) return cudaSuccess;
   // the band (exact zeros below it) decides the path and the blocks multiplied
-  lower_band_kernel<<<div_up((int64_t)n * 32, 256), 256, 0, s>>>(A, n, info_dev + 1);
-  e = sf_launched(1);
-  if (e != cudaSuccess) return e;
-  int bw = 0;
-  e = cudaMemcpyAsync(&bw, info_dev + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
-  if (e != cudaSuccess) return e;
-  e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return e;
+  int bw = std::min(bw_known, n - 1);
+  if (bw_known < 0) {
+    lower_band_kernel<<<div_up((int64_t)n * 32, 256), 256, 0, s>>>(A, n, info_dev + 1);
+    e = sf_launched(1);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(&bw, info_dev + 1, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+  }
   bw = std::max(bw, 0);
   if (band_tiles(bw) <= kBandMaxTiles) return band_chol_inverse(A, n, bw, dinv, out, info_dev, s);
   const int64_t nn = (int64_t)n * n;

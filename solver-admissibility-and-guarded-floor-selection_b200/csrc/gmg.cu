@@ -374,6 +374,28 @@ Gmg* gmg_create(Mesh* m, const simpfem_gmg_opts& o) {
         idx.push_back((int32_t)d);
       }
     G->nc = (int)idx.size();
+    // the dense coarsest matrix's structural lower bandwidth: the widest reach
+    // of the 27-point stencil in the compact (order-preserving) numbering; its
+    // values can only be zero farther out, so the factorisation needs no scan
+    {
+      const int NY = C.g.ny + 1, NZ = C.g.nz + 1;
+      int bw = 0;
+      for (int64_t d = 0; d < C.g.ndof; ++d) {
+        if (didx[d] < 0) continue;
+        const int64_t node = d / 3;
+        const int k = (int)(node % NZ), j = (int)((node / NZ) % NY), i = (int)(node / ((int64_t)NZ * NY));
+        for (int o = 0; o < 27; ++o) {
+          const int mi = i + o / 9 - 1, mj = j + (o / 3) % 3 - 1, mk = k + o % 3 - 1;
+          if (mi < 0 || mj < 0 || mk < 0 || mi > C.g.nx || mj > C.g.ny || mk > C.g.nz) continue;
+          const int64_t m = ((int64_t)mi * NY + mj) * NZ + mk;
+          for (int c = 0; c < 3; ++c) {
+            const int32_t q = didx[3 * m + c];
+            if (q >= 0) bw = std::max(bw, didx[d] - q);
+          }
+        }
+      }
+      G->c_bw = bw;
+    }
     G->c_idx.alloc(4 * std::max<size_t>(1, idx.size()));
     G->c_didx.alloc(4 * didx.size());
     if (!idx.empty()) SF_CUDA(cudaMemcpy(G->c_idx.p, idx.data(), 4 * idx.size(), cudaMemcpyHostToDevice));
@@ -1165,7 +1187,8 @@ static void setup_coarsest(Gmg& G) {
       SF_CUDA(launch_stencil_to_dense(L.g, L.K64.as<double>(), G.c_didx.as<int32_t>(), n, G.Adense.as<double>(),
                                       G.st));
       if (eps > 0) SF_CUDA(launch_add_diag(G.Adense.as<double>(), n, eps, G.st));
-      SF_CUDA(chol_inverse(G.Adense.as<double>(), n, G.Linv.as<double>(), G.cdinv.as<double>(), out, info, G.st));
+      SF_CUDA(chol_inverse(G.Adense.as<double>(), n, G.Linv.as<double>(), G.cdinv.as<double>(), out, info, G.st,
+                           G.c_bw));
       int h = 0;
       SF_CUDA(cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, G.st));
       SF_CUDA(cudaStreamSynchronize(G.st));

@@ -191,6 +191,7 @@ struct Gmg {
   int coarse_mode = 0;
   bool coarse_reg = false;
   int nc = 0;
+  int c_bw = -1;  // structural lower bandwidth of the dense coarsest matrix
   DevBuf c_idx, c_didx, Adense, Linv, LinvT, cb, cx, ctmp, cinfo;
   DevBuf LinvF, LinvTF;  // FP32 copies of Linv and LinvT read by the mixed cycle
   DevBuf cdinv;          // inverses of the diagonal tiles of the coarsest factor (scratch)

@@ -205,15 +205,16 @@ size_t band_dinv_bytes(int n);  // scratch of the band path: the inverses of L's
 cudaError_t band_chol_inverse(double* A, int n, int bw, double* dinv, const BandInvOut& out, int* info,
                               cudaStream_t s);
 // L^{-1} of the Cholesky factor of the SPD row-major A (destroyed) into the
-// requested outputs.  The lower bandwidth bw of A is measured (one stream
-// synchronisation); with ceil(bw / 32) <= kBandMaxTiles the band path writes
+// requested outputs.  The lower bandwidth bw of A is bw_known when that is >= 0
+// (a structural bound: A is zero farther below the diagonal), else it is
+// measured (one stream synchronisation); with ceil(bw / 32) <= kBandMaxTiles the band path writes
 // the outputs directly, else the recursion in dense.cu factors into work64
 // (n x n FP64) and the outputs are copied / transposed / converted from it.
 // info_dev[0]: 0, or the 1-based index of the first non-positive pivot, or
 // n + 1 when L^{-1} holds a non-finite entry; info_dev[1] is scratch.  dinv:
 // band_dinv_bytes(n) of scratch.
 cudaError_t chol_inverse(double* A, int n, double* work64, double* dinv, const BandInvOut& out, int* info_dev,
-                         cudaStream_t s);
+                         cudaStream_t s, int bw_known = -1);
 // Linv <- L^{-1} (lower, zero upper): chol_inverse into a zeroed Linv.
 cudaError_t dense_chol_inverse(double* A, int n, double* Linv, double* dinv, int* info_dev, cudaStream_t s);
 cudaError_t launch_coarsest_solve(const double* Linv, const double* LinvT, int n, const double* b,

@@ -24,8 +24,8 @@
 //    the diagonal tiles are kept for step 2.
 // 2. band_inverse_kernel: X = L^{-1} by 16-column blocks, independent of one
 //    another: X_JJ = L_JJ^{-1}, X_IJ = -L_II^{-1} sum_{K=max(J,I-WB)}^{I-1} L_IK X_KJ,
-//    the last WB tiles of the block kept in shared memory, the tiles of L and
-//    L_II^{-1} streamed through a cp.async ring, both products on the FP64 tensor
+//    the last WB tiles of the block kept in a power-of-two ring in shared
+//    memory, the tiles of L and L_II^{-1} streamed through a cp.async ring, both products on the FP64 tensor
 //    cores with four accumulator chains per warp.  Each CTA takes a long column
 //    block and its mirror so that every CTA walks ~NB tile rows.  It writes any
 //    of L^{-1} and L^{-T} in FP64 or FP32 directly (the mixed cycle reads only
@@ -401,15 +401,34 @@ __device__ void write_block(const double* X, int I, int c0, int n, const BandInv
   if (bad) atomicCAS(info, 0, n + 1);
 }
 
-// Order of the staged tiles of one column block (tile column J): for I = J+1 ..
-// NB-1 the tiles L_IK, K = max(J, I-WB) .. I-1, then L_II^{-1} (K == I).
-struct TileCursor {
+// Staged-tile stream of one column block (tile column J): for I = J+1 .. NB-1
+// the tiles L_IK, K = max(J, I-WB) .. I-1, then L_II^{-1} (K == I).  The copy
+// addresses of this thread are precomputed once; a tile costs one base
+// address and a few adds.
+struct TileStream {
   int I, K, J, WB;
-  __device__ void start(int j, int wb) {
+  const double* A;
+  const double* dinv;
+  int n;
+  int64_t n8;           // 8 rows of A
+  int dst_l, dst_d;     // this thread's first shared-memory slot of an L tile / a L_II^{-1} tile
+  int row_l, col_l;     // this thread's first row and column in an L tile
+  int src_d;            // this thread's first element of a L_II^{-1} tile
+  __device__ void start(int j, int wb, const double* a, const double* di, int nn) {
     J = j;
     WB = wb;
     I = j + 1;
     K = max(J, I - WB);
+    A = a;
+    dinv = di;
+    n = nn;
+    n8 = 8 * (int64_t)nn;
+    const int t = threadIdx.x;
+    row_l = t >> 5;
+    col_l = t & 31;
+    dst_l = row_l * T36 + col_l;
+    dst_d = (t >> 4) * T36 + 2 * (t & 15);
+    src_d = (t >> 4) * 32 + 2 * (t & 15);
   }
   __device__ void next() {
     if (K == I) {
@@ -419,46 +438,43 @@ struct TileCursor {
       ++K;
     }
   }
-};
-
-__device__ __forceinline__ void issue_tile(double* st, const TileCursor& c, const double* __restrict__ A,
-                                           const double* __restrict__ dinv, int n) {
-  const int t = threadIdx.x;
-  if (c.K == c.I) {
-    const double* src = dinv + (int64_t)c.I * 1024;
+  // L rows 8u + row_l (u = 0..3) / L_II^{-1} rows 16u + (t >> 4) (u = 0, 1)
+  __device__ __forceinline__ void issue(double* st) const {
+    if (K == I) {
+      const double* src = dinv + (int64_t)I * 1024 + src_d;
+      cp_async16(st + dst_d, src);
+      cp_async16(st + dst_d + 16 * T36, src + 16 * 32);
+    } else {
+      const int r0 = TS * I + row_l;
+      const double* src = A + (int64_t)r0 * n + TS * K + col_l;
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int e = t + FT * u, r = e >> 4, cc = 2 * (e & 15);
-      cp_async16(st + r * T36 + cc, src + r * 32 + cc);
-    }
-  } else {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int e = t + FT * u, r = e >> 5, cc = e & 31, gr = TS * c.I + r;
-      const bool ok = gr < n;
-      cp_async8z(st + r * T36 + cc, ok ? A + (int64_t)gr * n + TS * c.K + cc : A, ok);
+      for (int u = 0; u < 4; ++u) {
+        const bool ok = r0 + 8 * u < n;
+        cp_async8z(st + dst_l + 8 * u * T36, ok ? src + u * n8 : A, ok);
+      }
     }
   }
-}
+};
 
 // Grid: one CTA per pair of column blocks (cb, NCB - 1 - cb).  Warp w owns the
 // 8 x 8 output block (w / 2, w % 2) of the 32 x 16 block of every tile row.
+// RM + 1: the ring's size, a power of two >= WB + 1.
 __global__ void __launch_bounds__(FT) band_inverse_kernel(const double* __restrict__ A,
                                                           const double* __restrict__ dinv, int n, int NB, int WB,
-                                                          BandInvOut out, int* __restrict__ info) {
+                                                          int RM, BandInvOut out, int* __restrict__ info) {
   extern __shared__ __align__(16) double sm[];
-  const int R = WB + 1;
-  double* ring = sm;                        // [R][32][SX]: X_KJ of the last R tile rows
-  double* stage = ring + R * 32 * SX;       // [NSLOT][32][T36]
-  double* sacc = stage + NSLOT * 32 * T36;  // [32][SX]
+  double* ring = sm;                             // [RM + 1][32][SX]: X_KJ of the recent tile rows
+  double* stage = ring + (RM + 1) * 32 * SX;     // [NSLOT][32][T36]
+  double* sacc = stage + NSLOT * 32 * T36;       // [32][SX]
   const int t = threadIdx.x, lane = t & 31, w = t >> 5, g = lane >> 2, q = lane & 3;
   const int ar = 8 * (w >> 1) + g, bcol = 8 * (w & 1);
+  const int a_off = ar * T36 + q, b_off = q * SX + bcol + g, c_off = ar * SX + bcol + 2 * q;
   const int NCB = (n + CW - 1) / CW;
   for (int pass = 0; pass < 2; ++pass) {
     const int cb = pass == 0 ? (int)blockIdx.x : NCB - 1 - (int)blockIdx.x;
     if (pass == 1 && cb <= (int)blockIdx.x) break;
     const int c0 = CW * cb, J = c0 / TS, h = (c0 / CW) & 1;
-    double* xj = ring + (J % R) * 32 * SX;
+    double* xj = ring + (J & RM) * 32 * SX;
     for (int e = t; e < 32 * CW; e += FT) {
       const int r = e >> 4, c = e & 15;
       xj[r * SX + c] = dinv[(int64_t)J * 1024 + r * 32 + CW * h + c];
@@ -466,61 +482,66 @@ __global__ void __launch_bounds__(FT) band_inverse_kernel(const double* __restri
     __syncthreads();
     write_block(xj, J, c0, n, out, info);
 
-    TileCursor pc, cc;
-    pc.start(J, WB);
-    cc.start(J, WB);
+    TileStream ps;
+    ps.start(J, WB, A, dinv, n);
 #pragma unroll 1
     for (int s = 0; s < NSLOT - 1; ++s) {
-      if (pc.I < NB) {
-        issue_tile(stage + s * 32 * T36, pc, A, dinv, n);
-        pc.next();
+      if (ps.I < NB) {
+        ps.issue(stage + s * 32 * T36);
+        ps.next();
       }
       cp_commit();
     }
     int slot = 0;
-    double acc[4][2] = {};  // four accumulator chains, summed at the tile row's end
-    while (cc.I < NB) {
-      cp_wait_ring();
-      __syncthreads();  // everyone's copies of this tile landed; the previous slot is consumed
-      if (pc.I < NB) {
-        issue_tile(stage + (slot == 0 ? NSLOT - 1 : slot - 1) * 32 * T36, pc, A, dinv, n);
-        pc.next();
+#pragma unroll 1
+    for (int I = J + 1; I < NB; ++I) {
+      double acc[4][2] = {};  // four accumulator chains, summed at the tile row's end
+      const int kb = max(J, I - WB);
+#pragma unroll 1
+      for (int K = kb; K <= I; ++K) {
+        cp_wait_ring();
+        __syncthreads();  // everyone's copies of this tile landed; the previous slot is consumed
+        if (ps.I < NB) {
+          ps.issue(stage + (slot == 0 ? NSLOT - 1 : slot - 1) * 32 * T36);
+          ps.next();
+        }
+        cp_commit();
+        const double* st = stage + slot * 32 * T36 + a_off;
+        slot = slot + 1 == NSLOT ? 0 : slot + 1;
+        if (K < I) {
+          const double* xk = ring + (K & RM) * 32 * SX + b_off;
+#pragma unroll
+          for (int ks = 0; ks < 8; ++ks) dmma(acc[ks & 3][0], acc[ks & 3][1], st[4 * ks], xk[4 * ks * SX]);
+        } else {
+          // X_IJ = -L_II^{-1} (sum over K of L_IK X_KJ)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) sacc[c_off + e] = (acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e]);
+          __syncthreads();
+          double y[4][2] = {};
+#pragma unroll
+          for (int ks = 0; ks < 8; ++ks)
+            dmma(y[ks & 3][0], y[ks & 3][1], -st[4 * ks], sacc[(4 * ks + q) * SX + bcol + g]);
+          double* xi = ring + (I & RM) * 32 * SX;
+#pragma unroll
+          for (int e = 0; e < 2; ++e) xi[c_off + e] = (y[0][e] + y[1][e]) + (y[2][e] + y[3][e]);
+          __syncthreads();
+          write_block(xi, I, c0, n, out, info);
+        }
       }
-      cp_commit();
-      const double* st = stage + slot * 32 * T36;
-      if (cc.K < cc.I) {
-        const double* xk = ring + (cc.K % R) * 32 * SX;
-#pragma unroll
-        for (int ks = 0; ks < 8; ++ks)
-          dmma(acc[ks & 3][0], acc[ks & 3][1], st[ar * T36 + 4 * ks + q], xk[(4 * ks + q) * SX + bcol + g]);
-      } else {
-        // X_IJ = -L_II^{-1} (sum over K of L_IK X_KJ)
-#pragma unroll
-        for (int e = 0; e < 2; ++e)
-          sacc[ar * SX + bcol + 2 * q + e] = (acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e]);
-        __syncthreads();
-        double y[4][2] = {};
-#pragma unroll
-        for (int ks = 0; ks < 8; ++ks)
-          dmma(y[ks & 3][0], y[ks & 3][1], -st[ar * T36 + 4 * ks + q], sacc[(4 * ks + q) * SX + bcol + g]);
-        double* xi = ring + (cc.I % R) * 32 * SX;
-#pragma unroll
-        for (int e = 0; e < 2; ++e) xi[ar * SX + bcol + 2 * q + e] = (y[0][e] + y[1][e]) + (y[2][e] + y[3][e]);
-        __syncthreads();
-        write_block(xi, cc.I, c0, n, out, info);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[c][0] = acc[c][1] = 0.0;
-      }
-      slot = slot + 1 == NSLOT ? 0 : slot + 1;
-      cc.next();
     }
     cp_wait_all();
     __syncthreads();
   }
 }
 
+int ring_mask(int WB) {
+  int r = 1;
+  while (r < WB + 1) r <<= 1;
+  return r - 1;
+}
+
 size_t inverse_smem(int WB) {
-  return sizeof(double) * ((size_t)(WB + 1) * 32 * SX + NSLOT * 32 * T36 + 32 * SX);
+  return sizeof(double) * ((size_t)(ring_mask(WB) + 1) * 32 * SX + NSLOT * 32 * T36 + 32 * SX);
 }
 
 }  // namespace
@@ -558,7 +579,7 @@ cudaError_t band_chol_inverse(double* A, int n, int bw, double* dinv, const Band
     attr_done = true;
   }
   const int ncb = (n + CW - 1) / CW;
-  band_inverse_kernel<<<(ncb + 1) / 2, FT, inverse_smem(WB), s>>>(A, dinv, n, NB, WB, out, info);
+  band_inverse_kernel<<<(ncb + 1) / 2, FT, inverse_smem(WB), s>>>(A, dinv, n, NB, WB, ring_mask(WB), out, info);
   return sf_launched(1);
 }
 

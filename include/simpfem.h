@@ -355,7 +355,10 @@ int simpfem_policy_batch(const simpfem_policy_opts* o, const simpfem_policy_stat
  * GalerkinMatFreeGMG.setup (gpu_fem/multigrid_v4.py:1308-1337); the coarse solve
  * (gpu_fem/multigrid_v4.py:1916-1917) then multiplies by L^{-1} and L^{-T}.
  * *info_host: 0 on success, else the 1-based index of the first non-positive or
- * non-finite pivot, or n + 1 when L^{-1} holds a non-finite entry. */
+ * non-finite pivot, or n + 1 when L^{-1} holds a non-finite entry.  The lower
+ * bandwidth is measured from the data: up to 24 tiles of 32 (768) the band path
+ * runs (one 8-CTA thread-block cluster for the factor, one launch for L^{-1}),
+ * wider matrices take a recursive blocked factorisation. */
 int simpfem_dense_cholesky_inverse(int n, double* A, double* Linv, int* info_host, void* stream);
 
 /* ---- SIMP loop around the guarded solve ------------------------------------------

@@ -37,6 +37,9 @@
 // in dense.cu does; the caller regularises and refactors.
 #include <cooperative_groups.h>
 
+#include <map>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace cg = cooperative_groups;
@@ -547,6 +550,34 @@ size_t inverse_smem(int WB) {
 }  // namespace
 
 int band_tiles(int bw) { return (std::max(bw, 0) + TS - 1) / TS; }
+
+// Whether the current device can run the factorisation cluster at all (it can on
+// a whole B200; a partitioned or smaller device may not): asked once per device.
+bool band_path_available() {
+  static std::mutex mu;
+  static std::map<int, bool> known;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto it = known.find(dev);
+  if (it != known.end()) return it->second;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CL);
+  cfg.blockDim = dim3(FT);
+  cfg.dynamicSmemBytes = sizeof(double) * CholSmem::TOTAL;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  const bool ok = cudaOccupancyMaxActiveClusters(&clusters, band_chol_kernel, &cfg) == cudaSuccess && clusters > 0;
+  if (!ok) cudaGetLastError();
+  known[dev] = ok;
+  return ok;
+}
 
 size_t band_dinv_bytes(int n) { return sizeof(double) * 1024 * (size_t)std::max(1, (n + TS - 1) / TS); }
 

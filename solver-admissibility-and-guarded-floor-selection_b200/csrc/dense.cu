@@ -378,7 +378,8 @@ cudaError_t chol_inverse(double* A, int n, double* work64, double* dinv, const B
     if (e != cudaSuccess) return e;
   }
   bw = std::max(bw, 0);
-  if (band_tiles(bw) <= kBandMaxTiles) return band_chol_inverse(A, n, bw, dinv, out, info_dev, s);
+  if (band_tiles(bw) <= kBandMaxTiles && band_path_available())
+    return band_chol_inverse(A, n, bw, dinv, out, info_dev, s);
   const int64_t nn = (int64_t)n * n;
   e = cudaMemsetAsync(work64, 0, sizeof(double) * (size_t)nn, s);
   if (e != cudaSuccess) return e;

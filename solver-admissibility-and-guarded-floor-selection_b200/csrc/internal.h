@@ -201,6 +201,7 @@ struct BandInvOut {
 // The band path (bandchol.cu) takes matrices with ceil(bw / 32) <= kBandMaxTiles.
 constexpr int kBandMaxTiles = 24;
 int band_tiles(int bw);
+bool band_path_available();  // the device can run the band path's 8-CTA cluster
 size_t band_dinv_bytes(int n);  // scratch of the band path: the inverses of L's diagonal tiles
 cudaError_t band_chol_inverse(double* A, int n, int bw, double* dinv, const BandInvOut& out, int* info,
                               cudaStream_t s);

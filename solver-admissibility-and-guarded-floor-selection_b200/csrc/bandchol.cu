@@ -602,13 +602,12 @@ cudaError_t band_chol_inverse(double* A, int n, int bw, double* dinv, const Band
   if (e != cudaSuccess) return e;
   e = sf_launched(1);
   if (e != cudaSuccess) return e;
-  static bool attr_done = false;
-  if (!attr_done) {
-    e = cudaFuncSetAttribute(band_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)inverse_smem(kBandMaxTiles));
-    if (e != cudaSuccess) return e;
-    attr_done = true;
-  }
+  static std::atomic<uint64_t> attr_done;
+  e = once_per_device(attr_done, [] {
+    return cudaFuncSetAttribute(band_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)inverse_smem(kBandMaxTiles));
+  });
+  if (e != cudaSuccess) return e;
   const int ncb = (n + CW - 1) / CW;
   band_inverse_kernel<<<(ncb + 1) / 2, FT, inverse_smem(WB), s>>>(A, dinv, n, NB, WB, ring_mask(WB), out, info);
   return sf_launched(1);

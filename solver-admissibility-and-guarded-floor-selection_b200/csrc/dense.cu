@@ -189,12 +189,12 @@ cudaError_t dgemm(const DGemm& g, int tb, cudaStream_t s) {
   if (g.M <= 0 || g.N <= 0) return cudaSuccess;
   const dim3 grid(div_up(g.N, GN), div_up(g.M, GM));
   const size_t smem = sizeof(double) * NSTAGE * (A_STAGE + (tb ? B_STAGE_T : B_STAGE_N));
-  static bool attr_done[2] = {false, false};
-  if (!attr_done[tb]) {
-    if (tb == 0) cudaFuncSetAttribute(dgemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    else cudaFuncSetAttribute(dgemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_done[tb] = true;
-  }
+  static std::atomic<uint64_t> attr_done[2];
+  const cudaError_t ea = once_per_device(attr_done[tb], [&] {
+    return tb == 0 ? cudaFuncSetAttribute(dgemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                   : cudaFuncSetAttribute(dgemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
+  if (ea != cudaSuccess) return ea;
   if (tb == 0) dgemm_kernel<0><<<grid, GT, smem, s>>>(g);
   else dgemm_kernel<1><<<grid, GT, smem, s>>>(g);
   return sf_launched(1);

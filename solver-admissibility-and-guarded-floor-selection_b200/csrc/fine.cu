@@ -307,12 +307,12 @@ static cudaError_t launch_sweep(const Grid& g, const SweepShape& sh, const T* E,
   if (NT > MAXT || sh.bj < 2 || sh.bk < 2 || sh.cx < 1) return cudaErrorInvalidConfiguration;
   if ((int64_t)(sh.bj + 1) * 3 * (sh.bk + 1) > (int64_t)kTileLoads * NT) return cudaErrorInvalidConfiguration;
   const size_t smem = sweep_smem<T>(sh);
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(fine_sweep_kernel<T, EPI, KMODE, MAXT>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = true;
-  }
+  static std::atomic<uint64_t> attr_done;
+  const cudaError_t ea0 = once_per_device(attr_done, [] {
+    return cudaFuncSetAttribute(fine_sweep_kernel<T, EPI, KMODE, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                200 * 1024);
+  });
+  if (ea0 != cudaSuccess) return ea0;
   const int nbj = (g.ny + sh.bj - 1) / (sh.bj - 1);
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
   dim3 grid(nbj * nbk, div_up(g.nx + 1, sh.cx));
@@ -538,15 +538,15 @@ static cudaError_t launch_sweep_f32(const Grid& g, const SweepShape& sh, const f
   if (sh.variant == 1 || !x2_shape_ok(g, sh)) return launch_sweep<float, EPI, 0, 512>(g, sh, E, mask, u, ea, s);
   const int NT = sh.bj * sh.bk / 2, NE = sh.bj * sh.bk;
   const size_t smem = sizeof(float) * (36 * (size_t)NE + 9 * (size_t)(sh.bj + 1) * (sh.bk + 2));
-  static bool attr_done[2] = {false, false};
+  static std::atomic<uint64_t> attr_done[2];
   const int capped = sh.variant == 2 ? 1 : 0;
-  if (!attr_done[capped]) {
-    if (capped)
-      cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    else
-      cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done[capped] = true;
-  }
+  const cudaError_t ea0 = once_per_device(attr_done[capped], [&] {
+    return capped ? cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024)
+                  : cudaFuncSetAttribute(fine_sweep_x2_kernel<EPI, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024);
+  });
+  if (ea0 != cudaSuccess) return ea0;
   const int nbj = (g.ny + sh.bj - 1) / (sh.bj - 1);
   const int nbk = (g.nz + sh.bk - 1) / (sh.bk - 1);
   dim3 grid(nbj * nbk, div_up(g.nx + 1, sh.cx));

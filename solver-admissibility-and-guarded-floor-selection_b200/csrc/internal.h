@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -261,6 +262,22 @@ cudaError_t launch_select_vec(DType t, int64_t n, const void* trial, const void*
 
 // launch accounting: every launcher reports its kernel launches here
 cudaError_t sf_launched(int k);
+
+// Runs set() (a kernel attribute, say) the first time it is asked for the
+// current device; `done` holds one bit per device.  Two host threads may both
+// run it the first time -- harmless -- but none launches before its own call
+// returned.
+template <class F>
+inline cudaError_t once_per_device(std::atomic<uint64_t>& done, F&& set) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
+  if (bit != 0 && (done.load(std::memory_order_acquire) & bit) != 0) return cudaSuccess;
+  e = set();
+  if (e == cudaSuccess && bit != 0) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
 int64_t sf_launch_count();
 
 // error plumbing

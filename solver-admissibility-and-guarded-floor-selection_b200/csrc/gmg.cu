@@ -1168,7 +1168,9 @@ static void setup_coarsest(Gmg& G) {
   if (n <= G.o.dense_chol_max && n > 0) {
     const size_t nn = (size_t)n * n;
     G.Adense.alloc(8 * nn);
-    G.Linv.alloc(8 * nn);  // the FP64 cycle's L^{-1}; the wide-band recursion's work array
+    // the FP64 cycle's L^{-1}; otherwise only the wide-band recursion's work array
+    const bool band = band_tiles(G.c_bw) <= kBandMaxTiles && band_path_available();
+    if (G.cyc != F32 || !band) G.Linv.alloc(8 * nn);
     G.cdinv.alloc(band_dinv_bytes(n));
     BandInvOut out;
     if (G.cyc == F32) {

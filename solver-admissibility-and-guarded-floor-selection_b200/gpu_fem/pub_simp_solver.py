@@ -12,12 +12,16 @@ Names and semantics follow the reference's ``gpu_fem/pub_simp_solver.py``:
 * ``_build_density_filter`` (:215-243): cone filter, weights rmin - dist for
   element centroids closer than rmin, rows normalised to sum to one.
 * ``_heaviside`` (:245-253).
+* ``StepState`` (:116-135): the per-iteration state a SIMP parameter
+  controller reads.
 
 The CUDA operator does not use the edof table (node indices are computed from
 the grid position); it is provided for callers of the reference API.
 """
 
 from __future__ import annotations
+
+from dataclasses import dataclass, field
 
 import numpy as np
 import scipy.sparse as sp
@@ -123,3 +127,31 @@ def _heaviside(rho_f, beta, eta):
     return (np.tanh(beta * eta) + np.tanh(beta * (rho_f - eta))) / (
         np.tanh(beta * eta) + np.tanh(beta * (1.0 - eta))
     )
+
+
+@dataclass
+class StepState:
+    """What a parameter controller sees after each SIMP iteration: the iteration's
+    compliance and the best valid design so far, the physical design's volume
+    fraction, grayness 4 mean(rho (1 - rho)) and checkerboard measure, the
+    compliance's relative changes, the continuation parameters after the beta
+    schedule, and the convergence flags."""
+    iteration: int
+    compliance: float
+    best_compliance: float
+    best_iteration: int
+    volume_fraction: float
+    grayness: float
+    best_grayness: float
+    checkerboard: float
+    obj_slope: float
+    rel_change_1: float
+    rel_change_5: float
+    stagnation_counter: int
+    penal: float
+    rmin: float
+    move: float
+    beta: float
+    converged: bool
+    best_is_valid: bool
+    compliance_history: list = field(default_factory=list)

@@ -6,9 +6,9 @@ above themselves (run_gmg_floor_detector_prospective.py:18-24), put <root>/src
 first on sys.path and import gpu_fem and cupy from there.  Checked here without
 a GPU: the runner stand-in hands out this library's _build_components, and the
 cupy stand-in has the surface those drivers use.  With SIMPFEM_REFERENCE_ROOT
-set to a reference checkout, each of the four drivers is also placed, unchanged,
-in a copy of the drop-in tree and its own loader and imports are run: they must
-resolve to this library."""
+set to a reference checkout, each of the four detector drivers and the SIMP
+trajectory driver is also placed, unchanged, in a copy of the drop-in tree and
+its own loader and imports are run: they must resolve to this library."""
 
 import json
 import os
@@ -88,3 +88,28 @@ print(json.dumps({{"same": runner._build_components is p4._build_components,
     assert r["same"]
     assert r["fgmres"] == os.path.join(PKG, "multigrid_v4.py")
     assert r["cupy"] == os.path.realpath(os.path.join(DROP, "src", "cupy", "__init__.py"))
+
+
+@pytest.mark.skipif(not os.environ.get("SIMPFEM_REFERENCE_ROOT"), reason="needs a reference checkout")
+def test_unchanged_trajectory_driver_resolves_here(tmp_path):
+    """run_simp_floor_trajectory.py imports the SIMP loop, the solver, the router
+    and the controller from gpu_fem (:34-39) and subclasses SolverV4 (:65)."""
+    driver = "run_simp_floor_trajectory.py"
+    src = os.path.join(os.environ["SIMPFEM_REFERENCE_ROOT"], "experiments", "phase5", driver)
+    (tmp_path / "experiments" / "phase5").mkdir(parents=True)
+    shutil.copyfile(src, tmp_path / "experiments" / "phase5" / driver)
+    os.symlink(os.path.join(DROP, "src"), tmp_path / "src")
+    code = f"""
+import importlib.util, json, os
+spec = importlib.util.spec_from_file_location("drv", {str(tmp_path / "experiments" / "phase5" / driver)!r})
+d = importlib.util.module_from_spec(spec)
+spec.loader.exec_module(d)
+import gpu_fem.simp_gpu as sg, gpu_fem.solver_v4 as s4, gpu_fem.local_agents as la, gpu_fem.pub_baseline_controller as pc
+print(json.dumps({{"loop": d.run_simp_surrogate_gpu is sg.run_simp_surrogate_gpu and d.TO3DParams is sg.TO3DParams,
+                   "solver": issubclass(d.GuardedAdaptiveFloorSolverV4, s4.SolverV4),
+                   "agents": d.PureFEMRouter is la.PureFEMRouter and d.ScheduleOnlyController is pc.ScheduleOnlyController,
+                   "pkg": os.path.realpath(os.path.dirname(sg.__file__))}}))
+"""
+    r = _run(code)
+    assert r["loop"] and r["solver"] and r["agents"]
+    assert r["pkg"] == PKG

@@ -34,20 +34,35 @@ The returned ``rho_final`` / ``rho_best`` are numpy arrays, as the reference's
 are.  Only 3D meshes (nelz > 0) and solver classes of the matrix-free GMG path
 are on the accelerated solve; the reference's default ``GPUFEMSolver``
 (assembled CSR) is not provided.
+
+    python simp_gpu.py [--dims 200 100 50] [--iters 50] [--fine-smoother fp32]
+                       [--restart 100] [--controller none|schedule] [--out run.json]
+
+runs the loop on a cantilever of the given size with the in-loop guarded floor
+policy (floors 1e-12 | 1e-3, 1e-2; probe 100, r50 at 50; tol 1e-6), the call
+the trajectory driver makes, and prints the per-iteration record's summary.
 """
 
 from __future__ import annotations
 
+import argparse
+import json
 import math
+import os
+import sys
 import time
 from dataclasses import dataclass
 from typing import Callable, Optional
 
 import numpy as np
 
-from . import _lib
-from .pub_simp_solver import KE_UNIT_3D, StepState, _build_sparse_indices, _edof_table_3d
-from .simp_loop import OCUpdater, cone_filter, heaviside
+if __package__ in (None, ""):
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    __package__ = "gpu_fem"  # noqa: A001
+
+from . import _lib  # noqa: E402
+from .pub_simp_solver import KE_UNIT_3D, StepState, _build_sparse_indices, _edof_table_3d  # noqa: E402
+from .simp_loop import OCUpdater, cone_filter, heaviside  # noqa: E402
 
 
 @dataclass
@@ -299,3 +314,79 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
         "wall_time_sec": time.time() - t_start,
         "gpu_backend": getattr(solver, "_backend", "cupy"),
     }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description="run_simp_surrogate_gpu with the in-loop guarded floor policy")
+    ap.add_argument("--dims", type=int, nargs=3, default=[200, 100, 50])
+    ap.add_argument("--iters", type=int, default=50)
+    ap.add_argument("--penal", type=float, default=3.0)
+    ap.add_argument("--fine-smoother", default="fp32", choices=["fp64", "fp32"])
+    ap.add_argument("--smoother-type", default="chebyshev", choices=["chebyshev", "jacobi"])
+    ap.add_argument("--levels", type=int, default=4)
+    ap.add_argument("--restart", type=int, default=100)
+    ap.add_argument("--maxiter", type=int, default=300)
+    ap.add_argument("--heaviside", action="store_true", help="Heaviside projection (beta 1, doubled every 20)")
+    ap.add_argument("--controller", default="none", choices=["none", "schedule"])
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+
+    from .bc_generator import generate_bc
+    from .floor_trajectory import GuardedAdaptiveFloorSolverV4
+    from .local_agents import PureFEMRouter
+    from .presets import cantilever_spec
+    from .pub_baseline_controller import ScheduleOnlyController
+
+    nx, ny, nz = a.dims
+    spec = cantilever_spec(nx, ny, nz)
+    bc = generate_bc(spec)
+    params = TO3DParams(nelx=nx, nely=ny, nelz=nz, volfrac=spec.volfrac, penal=a.penal, emin=1e-12,
+                        rmin=spec.rmin if spec.rmin is not None else 1.5, max_iter=a.iters, min_iter=a.iters,
+                        use_heaviside=a.heaviside)
+    kw = dict(grid_dims=(nx, ny, nz), enable_warm_start=True, enable_matrix_free=True, enable_fused_cuda=False,
+              enable_matfree_gmg=True, matfree_gmg_levels=a.levels, gmg_fine_smoother=a.fine_smoother,
+              gmg_fine_degree=2, gmg_outer_solver="fgmres", gmg_restart=a.restart, gmg_smoother_type=a.smoother_type,
+              gmg_cycle_type="v", cg_tol=1e-6, cg_maxiter=a.maxiter, guarded_base_rho_min=1e-12,
+              guarded_ladder=(1e-3, 1e-2), guarded_probe_iters=100, guarded_probe_r50=50)
+
+    def show(st):
+        print(f"iter {st['iteration']:3d}  C={st['compliance']:.6g}  gray={st['grayness']:.4f}  "
+              f"floor={st['selected_rho_min']:.0e}  {st['policy_trigger']}  its={st['cg_iters']}  "
+              f"r={st['solver_true_rel_residual']:.2e}", flush=True)
+
+    torch = _lib.require_cuda()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = run_simp_surrogate_gpu(params, bc.fixed_dofs, bc.free_dofs, bc.F, bc.ndof, None, PureFEMRouter(),
+                                 param_controller=ScheduleOnlyController() if a.controller == "schedule" else None,
+                                 progress_callback=show, solver_class=GuardedAdaptiveFloorSolverV4,
+                                 solver_kwargs=kw)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    log = res["params_log"]
+    walls = [row["iter_wall_sec"] for row in log]
+    its = [row["cg_iters"] for row in log]
+    floors: dict = {}
+    for row in log:
+        key = f"{row['selected_rho_min']:.0e}"
+        floors[key] = floors.get(key, 0) + 1
+    summary = {
+        "dims": [nx, ny, nz], "elements": nx * ny * nz, "iterations": res["n_iter"], "wall_s": wall,
+        "first_iteration_s": walls[0] if walls else None,
+        "median_iteration_s": float(np.median(walls[1:])) if len(walls) > 1 else None,
+        "compliance_first_last": [log[0]["compliance"], log[-1]["compliance"]] if log else None,
+        "outer_iterations_median": float(np.median(its)) if its else None,
+        "outer_iterations_range": [min(its), max(its)] if its else None,
+        "floor_counts": floors,
+        "max_true_rel_residual": max(row["solver_true_rel_residual"] for row in log) if log else None,
+        "fine_smoother": a.fine_smoother, "smoother_type": a.smoother_type, "restart": a.restart,
+        "controller": a.controller, "heaviside": bool(a.heaviside),
+    }
+    print(json.dumps(summary))
+    if a.out:
+        with open(a.out, "w") as fh:
+            json.dump({"summary": summary, "params_log": log}, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()

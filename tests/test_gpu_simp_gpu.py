@@ -1,5 +1,7 @@
 """The SIMP loop entry (gpu_fem.simp_gpu.run_simp_surrogate_gpu) on the GPU
-against the reference trajectory driver's own runs.
+against the reference trajectory driver's own runs, and against the reference's
+own entry on the branches that driver does not reach (unprojected OC step,
+passive mask, surrogate and router hooks, plain SolverV4).
 
 The call is the one run_simp_floor_trajectory.py makes (_run_case, :277-352,
 with _solver_kwargs, :244-275): cantilever_3d (24x12x6), SIMP penal 4.5 at the
@@ -137,3 +139,89 @@ def test_fixed_floor_trajectory_matches_reference(cuda):
     assert result["best_is_valid"] == (summary["best_is_valid"] == "True")
     ref_rho = np.load(os.path.join(GOLDEN, "trajectory_driver_cantilever_3d.npz"))["fixed_rho_final"]
     assert np.linalg.norm(result["rho_final"] - ref_rho) <= env["rho"] * np.linalg.norm(ref_rho)
+
+
+def _entry_passive_mask(nx, ny, nz):
+    """The passive mask of make_simp_entry_golden.py: 2 solid, 1 void."""
+    m = np.zeros((nx, ny, nz), dtype=np.int32)
+    m[20:24, 4:8, :] = 2
+    m[8:12, 0:4, 0:3] = 1
+    return m.ravel()
+
+
+class _EchoSurrogate:
+    """The generator's surrogate: predicts the sensitivity of the last solve."""
+
+    uncertainty = 0.0
+
+    def __init__(self):
+        self._dc = None
+
+    @property
+    def is_ready(self):
+        return self._dc is not None
+
+    def update(self, rho_phys, rho_f, penal, iter_ratio, dc_phys):
+        self._dc = dc_phys.clone() if hasattr(dc_phys, "clone") else np.array(dc_phys, copy=True)
+
+    def predict(self, rho_phys, rho_f, penal, iter_ratio):
+        return self._dc, 0.0
+
+
+def _every_third_router(iteration, uncertainty, surrogate_ready, beta=1.0, **kwargs):
+    return iteration % 3 != 0
+
+
+def run_entry_branches():
+    """The unprojected OC step, a passive mask and the surrogate / router hooks
+    through run_simp_surrogate_gpu with plain SolverV4, as the golden generator
+    calls the reference's."""
+    from gpu_fem.bc_generator import generate_bc
+    from gpu_fem.presets import get_preset
+    from gpu_fem.simp_gpu import TO3DParams, run_simp_surrogate_gpu
+    from gpu_fem.solver_v4 import SolverV4
+
+    spec = get_preset("cantilever_3d")
+    nx, ny, nz = spec.nelx, spec.nely, spec.nelz
+    bc = generate_bc(spec)
+    params = TO3DParams(nelx=nx, nely=ny, nelz=nz, volfrac=spec.volfrac, penal=3.0, emin=1e-9, rmin=1.5,
+                        max_iter=12, min_iter=12, use_heaviside=False)
+    kw = dict(grid_dims=(nx, ny, nz), enable_warm_start=True, enable_matrix_free=True, enable_fused_cuda=False,
+              enable_matfree_gmg=True, matfree_gmg_levels=3, gmg_fine_smoother="fp64", gmg_fine_degree=2,
+              gmg_outer_solver="fgmres", gmg_restart=300, gmg_smoother_type="chebyshev", gmg_cycle_type="v",
+              cg_tol=1e-6, cg_maxiter=150, enable_profiling=False)
+    return run_simp_surrogate_gpu(params, bc.fixed_dofs.astype(np.int32), bc.free_dofs.astype(np.int32), bc.F,
+                                  bc.ndof, _EchoSurrogate(), _every_third_router, device="auto",
+                                  passive_mask=_entry_passive_mask(nx, ny, nz), solver_class=SolverV4,
+                                  solver_kwargs=kw)
+
+
+def test_entry_branches_match_reference(cuda):
+    """tests/golden/simp_entry_cantilever_3d.npz (make_simp_entry_golden.py):
+    the reference's own run_simp_surrogate_gpu with the unprojected OC step, a
+    passive mask, and a surrogate taking iterations 3, 6, 9, 12.  The same
+    surrogate flags, solve and surrogate counts, outer iteration counts within
+    2, every solve's FP64 true residual at or below 1e-6, and compliance,
+    change, volume, grayness and rho_final (the last filtered design: no design
+    passes the best-design gate in 12 iterations) inside
+    100 times the reference's own deviation under a 1e-12 load perturbation,
+    floored at 1e-9."""
+    g = np.load(os.path.join(GOLDEN, "simp_entry_cantilever_3d.npz"))
+    res = run_entry_branches()
+    log = res["params_log"]
+    assert len(log) == int(g["base_n_iter"]) == res["n_iter"]
+    assert [row["used_surrogate"] for row in log] == list(g["base_used_surrogate"])
+    assert res["fem_calls"] == int(g["base_fem_calls"]) and res["surrogate_calls"] == int(g["base_surrogate_calls"])
+    assert res["best_is_valid"] == bool(g["base_best_is_valid"])
+    for k, row in enumerate(log):
+        assert abs(row["cg_iters"] - int(g["base_cg_iters"][k])) <= 2, (k, row["cg_iters"], g["base_cg_iters"][k])
+        assert row["solver_true_rel_residual"] <= 1e-6, k
+    for key in ("compliance", "change", "volume", "grayness"):
+        a, b = g[f"base_{key}"], g[f"pert_{key}"]
+        env = np.maximum(FLOOR, ENVELOPE * np.maximum.accumulate(np.abs(a - b) / np.abs(a)))
+        got = np.array([row[key] for row in log])
+        dev = np.abs(got - a) / np.abs(a)
+        assert np.all(dev <= env), (key, dev, env)
+    ref, pert = g["base_rho_final"], g["pert_rho_final"]
+    env = max(FLOOR, ENVELOPE * float(np.linalg.norm(pert - ref) / np.linalg.norm(ref)))
+    assert np.linalg.norm(res["rho_final"] - ref) <= env * np.linalg.norm(ref)

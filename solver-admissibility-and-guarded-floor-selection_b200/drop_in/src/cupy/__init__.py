@@ -3,7 +3,8 @@
 The drivers (run_gmg_floor_detector_prospective.py, _density_field.py,
 run_gmg_fixed_floor_controls.py, run_gmg_floor_rule_check.py) do their linear
 algebra through ``gpu_fem`` and ``_build_components``; cupy only builds the
-moduli, takes norms, synchronises and snapshots memory
+moduli, takes norms and dot products (read back with ``.get()``), synchronises
+and snapshots memory
 (run_gmg_floor_detector_prospective.py:101-112, :204-248).  Those drivers put
 ``<root>/src`` first on ``sys.path``; with this directory as that ``src``, their
 ``import cupy`` resolves here and the calls act on torch tensors on the current
@@ -33,8 +34,16 @@ def zeros(shape, dtype=float64):
     return torch.zeros(shape, dtype=dtype, device="cuda")
 
 
+class _DeviceScalar(torch.Tensor):
+    """A 0-d device result with cupy's ``.get()``, the copy to the host as a numpy
+    scalar (run_gmg_fixed_floor_controls.py:128 reads the compliance so)."""
+
+    def get(self):
+        return self.detach().cpu().numpy()
+
+
 def dot(a, b):
-    return torch.dot(a.reshape(-1), b.reshape(-1))
+    return torch.dot(a.reshape(-1), b.reshape(-1)).as_subclass(_DeviceScalar)
 
 
 def asnumpy(a):

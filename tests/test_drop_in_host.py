@@ -55,6 +55,9 @@ ok = ok and callable(cp.linalg.norm) and callable(cp.cuda.Stream.null.synchroniz
 ok = ok and callable(cp.cuda.runtime.memGetInfo)
 ok = ok and callable(cp.get_default_memory_pool().used_bytes) and callable(cp.get_default_memory_pool().total_bytes)
 ok = ok and cp.get_default_pinned_memory_pool().n_free_blocks() == 0
+import torch
+one = torch.ones(2, dtype=torch.float64)
+ok = ok and float(cp.dot(one, one).get()) == 2.0 and float(cp.dot(one, one)) == 2.0
 print(json.dumps({{"ok": ok, "file": cp.__file__}}))
 """
     r = _run(code)

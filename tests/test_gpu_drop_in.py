@@ -41,10 +41,12 @@ x, iters, conv = _cupy_fgmres(lambda v: mf_op.matvec(v, E_e), F_free_gpu, gmg.ap
                               restart=100)
 cp.cuda.Stream.null.synchronize()
 rel = float(cp.linalg.norm(F_free_gpu - mf_op.matvec(x, E_e)) / b_norm)
+compliance = float(cp.dot(F_free_gpu, x).get())
+direct = float((F_free_gpu * x).sum())
 free_b, total_b = cp.cuda.runtime.memGetInfo()
 used = cp.get_default_memory_pool().used_bytes()
 print(json.dumps({{"iters": int(iters), "conv": bool(conv), "rel": rel, "mem_ok": 0 < free_b <= total_b,
-                   "used": used, "cupy": cp.__file__}}))
+                   "used": used, "cupy": cp.__file__, "compliance": compliance, "direct": direct}}))
 """
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=900)
     assert out.returncode == 0, out.stderr[-3000:]
@@ -53,3 +55,4 @@ print(json.dumps({{"iters": int(iters), "conv": bool(conv), "rel": rel, "mem_ok"
     assert r["rel"] <= 1e-6
     assert r["mem_ok"] and r["used"] > 0
     assert r["cupy"].startswith(os.path.join(DROP, "src", "cupy"))
+    assert r["compliance"] > 0 and abs(r["compliance"] - r["direct"]) <= 1e-12 * r["direct"]

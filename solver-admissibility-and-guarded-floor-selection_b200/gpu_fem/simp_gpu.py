@@ -23,15 +23,15 @@ fields resident on the device:
   compliance change across the window < compliance_tol, iteration >= min_iter,
   :488-495), beta doubled every 20 iterations (:497-499), and the controller's
   action on a ``StepState``: penal clipped to [1, 5], rmin to [1.1, 4], move to
-  [0.03, 0.4], beta to [1, 64], a restart from the best design; a controller
-  that raises leaves the parameters as they were, as in the reference
-  (:501-535);
+  [0.03, 0.4], beta to [1, 64], a restart from the best design; when the
+  controller raises, the rest of its action is skipped, as in the reference
+  (:501-535), with a RuntimeWarning here;
 * per iteration one ``params_log`` row and one ``progress_callback`` state with
   the reference's keys in its order, the solver's ``last_*`` attributes (floor,
   trigger, probe read-outs, FP64 true residual) included (:537-590).
 
 The returned ``rho_final`` / ``rho_best`` are numpy arrays, as the reference's
-are.  Only 3D meshes (nelz > 0) and solver classes of the matrix-free GMG path
+are; ``fixed`` is accepted for the signature (the solver takes the free DOFs).  Only 3D meshes (nelz > 0) and solver classes of the matrix-free GMG path
 are on the accelerated solve; the reference's default ``GPUFEMSolver``
 (assembled CSR) is not provided.
 
@@ -51,6 +51,7 @@ import math
 import os
 import sys
 import time
+import warnings
 from dataclasses import dataclass
 from typing import Callable, Optional
 
@@ -260,8 +261,9 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
                     if action.get("restart", False) and best_is_valid:
                         rho_new = best_rho.clone()
                         solver.invalidate()
-            except Exception:
-                pass
+            except Exception as exc:  # the reference keeps going and skips the rest of the action
+                warnings.warn(f"SIMP parameter controller raised {exc!r} at iteration {iteration}; "
+                              "the rest of its action is skipped", RuntimeWarning, stacklevel=2)
 
         readouts = _solver_readouts(solver, Emin)
         uncertainty = surrogate.uncertainty if surrogate is not None else 0.0

@@ -92,6 +92,9 @@ class TO3DParams:
     amg_rebuild_tol: float = 0.15
 
 
+_DEVICE = "cuda"  # where the loop keeps its design fields
+
+
 def _grayness(x) -> float:
     return float(4.0 * (x * (1.0 - x)).mean())
 
@@ -122,6 +125,26 @@ def _solver_readouts(solver, emin: float) -> dict:
     }
 
 
+def _oc_step(oc, cache: dict, dims, rmin: float, rho, rho_f, dc, beta: float, eta: float, volfrac: float,
+             move: float, projected: bool):
+    """One OC update as _oc_step_cupy makes it (simp_gpu.py:212-294): with the
+    projection simpfem_oc_update_projected, without it simpfem_oc_update on H^T dc
+    with the volume weights H^T 1 (kept in ``cache`` for the current radius).
+    Returns (rho_new, change)."""
+    if projected:
+        rho_new, change, _, _ = oc.projected(dims, rmin, rho, rho_f, dc, beta, eta, volfrac, move)
+        return rho_new, change
+    weights = cache.get(rmin)
+    if weights is None:
+        torch = _lib.require_cuda()
+        weights = cone_filter(torch.ones(rho.numel(), dtype=torch.float64, device=_DEVICE), dims, rmin,
+                              transpose=True)
+        cache.clear()
+        cache[rmin] = weights
+    rho_new, change, _, _ = oc(rho, cone_filter(dc, dims, rmin, transpose=True), weights, volfrac, move)
+    return rho_new, change
+
+
 def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrogate, router: Callable,
                            device: str = "auto", param_controller: Optional[Callable] = None,
                            passive_mask=None, verbose: bool = False, progress_callback: Optional[Callable] = None,
@@ -150,10 +173,10 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
                           amg_ndof_threshold=params.amg_ndof_threshold, amg_rebuild_tol=params.amg_rebuild_tol,
                           **extra)
 
-    dev = dict(dtype=torch.float64, device="cuda")
+    dev = dict(dtype=torch.float64, device=_DEVICE)
     passive = None
     if passive_mask is not None:
-        pm = torch.as_tensor(np.asarray(passive_mask), device="cuda")
+        pm = torch.as_tensor(np.asarray(passive_mask), device=_DEVICE)
         passive = (pm == 1, pm == 2)
 
     def pin_passive(x):
@@ -167,7 +190,7 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
     beta, eta = float(params.beta_init), float(params.eta)
     prev_rmin = rmin
     oc = OCUpdater()
-    vol_weights = None  # H^T 1 at the current radius, for the unprojected OC step
+    vol_cache: dict = {}
 
     best_rho = rho.clone()
     best_compliance = math.inf
@@ -186,7 +209,6 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
         if abs(rmin - prev_rmin) > 1e-6:
             solver.invalidate()
             prev_rmin = rmin
-            vol_weights = None
 
         rho_f = cone_filter(rho, dims, rmin)
         projected = bool(params.use_heaviside) and beta > 1e-6
@@ -212,13 +234,8 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
         compliance = float(compliance)
         dc_dev = _lib.as_cuda(dc_phys, torch.float64)
 
-        if projected:
-            rho_new, change, _, _ = oc.projected(dims, rmin, rho, rho_f, dc_dev, beta, eta, params.volfrac, move)
-        else:
-            if vol_weights is None:
-                vol_weights = cone_filter(torch.ones(n_elem, **dev), dims, rmin, transpose=True)
-            dc_design = cone_filter(dc_dev, dims, rmin, transpose=True)
-            rho_new, change, _, _ = oc(rho, dc_design, vol_weights, params.volfrac, move)
+        rho_new, change = _oc_step(oc, vol_cache, dims, rmin, rho, rho_f, dc_dev, beta, eta, params.volfrac, move,
+                                   projected)
         rho_new = pin_passive(rho_new)
 
         gray_now = _grayness(rho_phys)

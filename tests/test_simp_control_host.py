@@ -113,3 +113,46 @@ def test_scenarios_reach_the_branches():
     assert restarts > 0 and ctl["scalars"]["best_is_valid"]
     assert plain["scalars"]["n_iter"] < fakes.SCENARIOS["plain"]["params"]["max_iter"]
     assert plain["params_log"][-1]["change"] < fakes.SCENARIOS["plain"]["params"]["tol"]
+
+
+def test_oc_step_wiring(monkeypatch):
+    """The real _oc_step: the projected form goes to simpfem_oc_update_projected with
+    the loop's arguments; the unprojected one to simpfem_oc_update with H^T dc and the
+    volume weights H^T 1, computed once per radius."""
+    from gpu_fem import simp_gpu
+
+    calls = []
+
+    def cone_filter(x, dims, rmin, transpose=False):
+        calls.append(("filter", rmin, transpose, float(x.sum())))
+        return x * (2.0 if transpose else 1.0)
+
+    class OC:
+        def projected(self, *args):
+            calls.append(("projected",) + tuple(a if not torch.is_tensor(a) else float(a.sum()) for a in args))
+            return torch.zeros(3), 0.5, 1.0, 7
+
+        def __call__(self, rho, dc_design, weights, volfrac, move):
+            calls.append(("oc", float(dc_design.sum()), float(weights.sum()), volfrac, move))
+            return torch.ones(3), 0.25, 1.0, 7
+
+    monkeypatch.setattr(simp_gpu, "_lib", types.SimpleNamespace(require_cuda=lambda: torch, as_cuda=_host_tensor))
+    monkeypatch.setattr(simp_gpu, "_DEVICE", "cpu")
+    monkeypatch.setattr(simp_gpu, "cone_filter", cone_filter)
+    rho, rho_f, dc = torch.full((3,), 0.25, dtype=torch.float64), torch.full((3,), 0.5, dtype=torch.float64), \
+        torch.full((3,), -1.0, dtype=torch.float64)
+    cache = {}
+    out = simp_gpu._oc_step(OC(), cache, (3, 1, 1), 1.5, rho, rho_f, dc, 4.0, 0.5, 0.3, 0.2, True)
+    assert out[1] == 0.5 and calls[-1][0] == "projected" and calls[-1][1:] == ((3, 1, 1), 1.5, 0.75, 1.5, -3.0,
+                                                                                 4.0, 0.5, 0.3, 0.2)
+    assert not cache
+    calls.clear()
+    for rmin in (1.5, 1.5, 1.4):
+        rho_new, change = simp_gpu._oc_step(OC(), cache, (3, 1, 1), rmin, rho, rho_f, dc, 4.0, 0.5, 0.3, 0.2, False)
+        assert change == 0.25 and torch.equal(rho_new, torch.ones(3))
+    # weights H^T 1 for 1.5, then only H^T dc, then new weights for 1.4
+    assert [c[:3] for c in calls if c[0] == "filter"] == [
+        ("filter", 1.5, True), ("filter", 1.5, True), ("filter", 1.5, True), ("filter", 1.4, True),
+        ("filter", 1.4, True)]
+    assert [c for c in calls if c[0] == "oc"] == [("oc", -6.0, 6.0, 0.3, 0.2)] * 3
+    assert list(cache) == [1.4]

@@ -7,7 +7,10 @@ this file by path, two directories above their own, and call its
 this library's factory (``gpu_fem.paper4``): the same keyword arguments and the
 same 8-tuple, over torch CUDA tensors, with every kernel from libsimpfem.so.
 The other helpers of the reference runner that the drivers reach are exported
-alongside.
+alongside, among them the host-side mesh data the direct-solve drivers
+(run_direct_floor_atlas.py, run_direct_floor_conditioning.py,
+compare_reduced_floor_perturbation.py) assemble their sparse matrices from:
+``KE_UNIT_3D``, ``_edof_table_3d`` and ``_build_sparse_indices``.
 """
 
 from __future__ import annotations
@@ -28,3 +31,4 @@ from gpu_fem.paper4 import (  # noqa: E402,F401
     _fgmres,
     _pcg,
 )
+from gpu_fem.pub_simp_solver import KE_UNIT_3D, _build_sparse_indices, _edof_table_3d  # noqa: E402,F401

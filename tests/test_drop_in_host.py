@@ -116,3 +116,90 @@ print(json.dumps({{"loop": d.run_simp_surrogate_gpu is sg.run_simp_surrogate_gpu
     r = _run(code)
     assert r["loop"] and r["solver"] and r["agents"]
     assert r["pkg"] == PKG
+
+
+def _csv(path):
+    import csv
+
+    with open(path, newline="") as f:
+        return list(csv.DictReader(f))
+
+
+@pytest.mark.skipif(not os.environ.get("SIMPFEM_REFERENCE_ROOT"), reason="needs a reference checkout")
+def test_unchanged_direct_solve_drivers_match_reference(tmp_path):
+    """run_direct_floor_atlas.py, run_direct_floor_conditioning.py and
+    compare_reduced_floor_perturbation.py assemble K from the paper-4 runner's
+    KE_UNIT_3D, _edof_table_3d and _build_sparse_indices and solve it with scipy on
+    the host, so they run here without a GPU.  Unchanged, over the drop-in tree,
+    against their run over the reference's own package
+    (tests/golden/make_direct_floor_golden.py): the same rows, flags and counts; the
+    matrix diagonal to 1e-14 (the two element matrices differ in the last bits);
+    lambda_max to 1e-12; the solution norm, lambda_min and kappa within ten times the
+    row's own kappa * eps (at least 1e-8), the round-off a solve at that
+    conditioning carries; direct residuals below 1e-10; for the floor comparison,
+    compliances to 1e-8, the solution change against the 1e-12 solve within ten
+    times that solve's kappa * eps, and the raised solution's residual under the
+    1e-12 operator to 1e-6 (round-off level, below 1e-10, on the 1e-12 rows)."""
+    args = ["--preset", "cantilever_3d", "--probabilities", "0.2,0.35", "--rho-min-values", "1e-12,1e-6,1e-3",
+            "--seeds", "3", "--out-dir", str(tmp_path / "out")]
+    (tmp_path / "experiments" / "phase5").mkdir(parents=True)
+    os.symlink(os.path.join(DROP, "experiments", "paper4"), tmp_path / "experiments" / "paper4")
+    os.symlink(os.path.join(DROP, "src"), tmp_path / "src")
+    for driver in ("run_direct_floor_atlas.py", "run_direct_floor_conditioning.py",
+                   "compare_reduced_floor_perturbation.py"):
+        src = os.path.join(os.environ["SIMPFEM_REFERENCE_ROOT"], "experiments", "phase5", driver)
+        shutil.copyfile(src, tmp_path / "experiments" / "phase5" / driver)
+        out = subprocess.run([sys.executable, str(tmp_path / "experiments" / "phase5" / driver)] + args,
+                             capture_output=True, text=True, timeout=900)
+        assert out.returncode == 0, out.stderr[-2000:]
+    golden = os.path.join(REPO, "tests", "golden")
+    cond = _csv(os.path.join(golden, "direct_floor_conditioning_cantilever_3d.csv"))
+    kappa_eps = {(r["solid_probability"], r["rho_min"]): float(r["kappa_times_eps"]) for r in cond}
+
+    def close(a, b, rel, where):
+        a, b = float(a), float(b)
+        assert abs(a - b) <= rel * abs(b), (where, a, b, rel)
+
+    for mine, ref in (("direct_floor_atlas.csv", "direct_floor_atlas_cantilever_3d.csv"),
+                      ("direct_floor_conditioning.csv", "direct_floor_conditioning_cantilever_3d.csv")):
+        got, exp = _csv(tmp_path / "out" / mine), _csv(os.path.join(golden, ref))
+        assert len(got) == len(exp) and list(got[0]) == list(exp[0])
+        for g, r in zip(got, exp):
+            key = (r["solid_probability"], r["rho_min"])
+            loose = max(1e-8, 10.0 * kappa_eps[key])
+            for k in ("preset", "seed", "solid_probability", "rho_min", "penal", "tol", "converged", "n_free", "nnz"):
+                if k in r:
+                    assert g[k] == r[k], (mine, key, k)
+            for k in ("diag_min", "diag_max", "diag_ratio"):
+                if k in r:
+                    close(g[k], r[k], 1e-14, (mine, key, k))
+            if "lambda_max" in r:
+                close(g["lambda_max"], r["lambda_max"], 1e-12, (mine, key))
+            for k in ("x_norm", "lambda_min", "kappa"):
+                if k in r:
+                    close(g[k], r[k], loose, (mine, key, k))
+            assert float(g["rel_residual"]) <= 1e-10 and float(r["rel_residual"]) <= 1e-10
+    crit = _csv(tmp_path / "out" / "direct_floor_critical.csv")
+    exp = _csv(os.path.join(golden, "direct_floor_critical_cantilever_3d.csv"))
+    assert [{k: v for k, v in r.items() if not k.startswith("critical_rel") and k != "critical_x_norm"} for r in crit] \
+        == [{k: v for k, v in r.items() if not k.startswith("critical_rel") and k != "critical_x_norm"} for r in exp]
+    got = _csv(tmp_path / "out" / "reduced_floor_perturbation_summary.csv")
+    exp = _csv(os.path.join(golden, "reduced_floor_perturbation_cantilever_3d.csv"))
+    assert len(got) == len(exp) and list(got[0]) == list(exp[0])
+    for g, r in zip(got, exp):
+        key = (r["solid_probability"], r["rho_min"])
+        ref_noise = 10.0 * kappa_eps[(r["solid_probability"], "1e-12")]
+        for k in ("preset", "seed", "solid_probability", "n_elem", "n_free", "rho_min", "reference_rho_min", "penal",
+                  "solid_count", "solid_fraction"):
+            assert g[k] == r[k], (key, k)
+        for k in ("compliance", "reference_compliance"):
+            close(g[k], r[k], 1e-8, key)
+        assert abs(float(g["rel_compliance_change"]) - float(r["rel_compliance_change"])) <= 1e-8, key
+        assert abs(float(g["rel_u_error"]) - float(r["rel_u_error"])) <= ref_noise, key
+        for k in ("direct_rel_residual", "reference_direct_rel_residual"):
+            assert float(g[k]) <= 1e-10 and float(r[k]) <= 1e-10, (key, k)
+        k = "raised_solution_residual_under_reference_operator"
+        if float(r[k]) <= 1e-10:
+            assert float(g[k]) <= 1e-10, key
+        else:
+            close(g[k], r[k], 1e-6, key)

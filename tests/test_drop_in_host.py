@@ -203,3 +203,46 @@ def test_unchanged_direct_solve_drivers_match_reference(tmp_path):
             assert float(g[k]) <= 1e-10, key
         else:
             close(g[k], r[k], 1e-6, key)
+
+
+@pytest.mark.skipif(not os.environ.get("SIMPFEM_REFERENCE_ROOT"), reason="needs a reference checkout")
+def test_unchanged_direct_solve_drivers_reproduce_published_tables(tmp_path):
+    """The two direct-solve drivers, unchanged over the drop-in tree at the arguments
+    of the reference's published tables (tests/golden/published_direct_floor_*_seed19.csv,
+    from its data/analysis_tables; make_published_direct_floor.py): the atlas at its
+    defaults (seed 19, six solid probabilities, floors 1e-12 to 1e-3) gives the same
+    critical floor for every probability, with the solution norm there within 1e-5;
+    the conditioning sweep at seed 19 (48 rows, floors 1e-12 to 1e-2) the same
+    converged flag on every row, lambda_max to 1e-12 and lambda_min within the row's
+    own kappa * eps (at least 1e-8).  Residuals at these conditionings are round-off
+    and are compared through the flags."""
+    (tmp_path / "experiments" / "phase5").mkdir(parents=True)
+    os.symlink(os.path.join(DROP, "experiments", "paper4"), tmp_path / "experiments" / "paper4")
+    os.symlink(os.path.join(DROP, "src"), tmp_path / "src")
+    runs = {"run_direct_floor_atlas.py": [], "run_direct_floor_conditioning.py": ["--seeds", "19"]}
+    for driver, extra in runs.items():
+        shutil.copyfile(os.path.join(os.environ["SIMPFEM_REFERENCE_ROOT"], "experiments", "phase5", driver),
+                        tmp_path / "experiments" / "phase5" / driver)
+        out = subprocess.run([sys.executable, str(tmp_path / "experiments" / "phase5" / driver), *extra,
+                              "--out-dir", str(tmp_path / "out")], capture_output=True, text=True, timeout=1200)
+        assert out.returncode == 0, out.stderr[-2000:]
+    golden = os.path.join(REPO, "tests", "golden")
+    got = _csv(tmp_path / "out" / "direct_floor_critical.csv")
+    exp = _csv(os.path.join(golden, "published_direct_floor_critical_seed19.csv"))
+    assert len(got) == len(exp) == 6 and list(got[0]) == list(exp[0])
+    for g, r in zip(got, exp):
+        for k in ("preset", "seed", "solid_probability", "critical_rho_min", "all_failed"):
+            assert g[k] == r[k], (r["solid_probability"], k, g[k], r[k])
+        x, y = float(g["critical_x_norm"]), float(r["critical_x_norm"])
+        assert abs(x - y) <= 1e-5 * y, (r["solid_probability"], x, y)
+    got = _csv(tmp_path / "out" / "direct_floor_conditioning.csv")
+    exp = _csv(os.path.join(golden, "published_direct_floor_conditioning_seed19.csv"))
+    assert len(got) == len(exp) == 48 and list(got[0]) == list(exp[0])
+    for g, r in zip(got, exp):
+        key = (r["solid_probability"], r["rho_min"])
+        for k in ("preset", "seed", "solid_probability", "rho_min", "penal", "converged", "n_free"):
+            assert g[k] == r[k], (key, k, g[k], r[k])
+        lmax, lmax_ref = float(g["lambda_max"]), float(r["lambda_max"])
+        assert abs(lmax - lmax_ref) <= 1e-12 * lmax_ref, key
+        lmin, lmin_ref = float(g["lambda_min"]), float(r["lambda_min"])
+        assert abs(lmin - lmin_ref) <= max(1e-8, float(r["kappa_times_eps"])) * lmin_ref, (key, lmin, lmin_ref)

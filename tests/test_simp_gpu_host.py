@@ -51,6 +51,35 @@ def test_schedule_controller_replays_reference_runs():
             assert rmin == float(row["rmin"]), row["iteration"]
 
 
+def test_schedule_controller_replays_published_runs():
+    """The reference's published guarded trajectories (cantilever_gpu_medium and
+    bridge_gpu_medium, 40 iterations each; published_guarded_trajectories_iters.csv)
+    recorded the same continuation parameters after every iteration."""
+    from gpu_fem.pub_baseline_controller import ScheduleOnlyController
+    from gpu_fem.pub_simp_solver import StepState
+
+    with open(os.path.join(GOLDEN, "published_guarded_trajectories_iters.csv"), newline="") as f:
+        rows = list(csv.DictReader(f))
+    runs = {}
+    for row in rows:
+        runs.setdefault(row["run_id"], []).append(row)
+    assert len(runs) == 2 and all(len(r) == 40 for r in runs.values())
+    ctl = ScheduleOnlyController()
+    for run in runs.values():
+        rmin = 1.5
+        for row in run:
+            state = StepState(iteration=int(row["iteration"]), compliance=1.0, best_compliance=1.0, best_iteration=0,
+                              volume_fraction=0.3, grayness=0.5, best_grayness=0.5, checkerboard=0.0, obj_slope=0.0,
+                              rel_change_1=0.0, rel_change_5=0.0, stagnation_counter=0, penal=0.0, rmin=rmin,
+                              move=0.0, beta=0.0, converged=False, best_is_valid=False)
+            act = ctl(state, None)
+            rmin = float(np.clip(act.get("rmin", rmin), 1.1, 4.0))
+            assert (float(np.clip(act["penal"], 1.0, 5.0)), float(np.clip(act["beta"], 1.0, 64.0)),
+                    float(np.clip(act["move"], 0.03, 0.4)), rmin) == \
+                (float(row["penal"]), float(row["beta"]), float(row["move"]), float(row["rmin"])), \
+                (row["run_id"], row["iteration"])
+
+
 def test_schedule_controller_phases_and_restart():
     from gpu_fem.pub_baseline_controller import ScheduleOnlyController
     from gpu_fem.pub_simp_solver import StepState

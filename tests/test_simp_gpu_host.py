@@ -52,18 +52,19 @@ def test_schedule_controller_replays_reference_runs():
 
 
 def test_schedule_controller_replays_published_runs():
-    """The reference's published guarded trajectories (cantilever_gpu_medium and
-    bridge_gpu_medium, 40 iterations each; published_guarded_trajectories_iters.csv)
-    recorded the same continuation parameters after every iteration."""
+    """The reference's published trajectories on cantilever_gpu_medium and
+    bridge_gpu_medium, 40 iterations each -- guarded (published_guarded_trajectories_iters.csv)
+    and at fixed floors 1e-12, 1e-3, 1e-2 (published_fixed_floor_trajectories_*_iters.csv)
+    -- recorded the same continuation parameters after every iteration."""
     from gpu_fem.pub_baseline_controller import ScheduleOnlyController
     from gpu_fem.pub_simp_solver import StepState
 
-    with open(os.path.join(GOLDEN, "published_guarded_trajectories_iters.csv"), newline="") as f:
-        rows = list(csv.DictReader(f))
     runs = {}
-    for row in rows:
-        runs.setdefault(row["run_id"], []).append(row)
-    assert len(runs) == 2 and all(len(r) == 40 for r in runs.values())
+    for name in ("guarded_trajectories", "fixed_floor_trajectories_cantilever", "fixed_floor_trajectories_bridge"):
+        with open(os.path.join(GOLDEN, f"published_{name}_iters.csv"), newline="") as f:
+            for row in csv.DictReader(f):
+                runs.setdefault(row["run_id"], []).append(row)
+    assert len(runs) == 8 and all(len(r) == 40 for r in runs.values())
     ctl = ScheduleOnlyController()
     for run in runs.values():
         rmin = 1.5

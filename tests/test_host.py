@@ -127,3 +127,70 @@ def test_abi_rejects_bad_arguments_before_touching_the_device():
     assert st == 1 and "rmin" in msg
     st, msg = status("simpfem_cone_filter", 4, 4, 4, 1.5, 0, fake, fake, None)
     assert st == 1 and "cone_filter" in msg
+
+
+def test_every_entry_point_rejects_null_arguments_before_touching_the_device():
+    """Every status-returning entry point of include/simpfem.h checks its handles,
+    pointers and sizes before any CUDA call: with null arguments it returns
+    SIMPFEM_EINVAL (1) and a message naming the call; the destroy functions take
+    a null handle as a no-op (SIMPFEM_OK)."""
+    import ctypes
+
+    from gpu_fem import _lib
+
+    lib = _lib.load()
+    out = ctypes.c_void_p()
+    o = ctypes.byref(out)
+    N = None
+    cases = {
+        "simpfem_gmg_time_smoother_step": ((N, 0, 0, N, N), "time_smoother_step"),
+        "simpfem_gmg_time_operator": ((N, 0, N, N), "time_operator"),
+        "simpfem_mesh_create": ((0, 0, 0, N, 0, N, o), "mesh_create"),
+        "simpfem_mesh_info": ((N, N, N, N), "null mesh"),
+        "simpfem_mesh_tune": ((N, N), "null mesh"),
+        "simpfem_matvec": ((N, 0, N, N, N, N), "simpfem_matvec"),
+        "simpfem_matvec_full": ((N, 0, N, N, N, N), "simpfem_matvec_full"),
+        "simpfem_extract_diagonal": ((N, N, N, N), "extract_diagonal"),
+        "simpfem_node_blocks": ((N, N, N, N, N), "node_blocks"),
+        "simpfem_node_block_apply": ((N, N, N, N, N), "node_block_apply"),
+        "simpfem_element_energy": ((N, N, N, N), "element_energy"),
+        "simpfem_true_residual": ((N, N, N, N, N, N), "true_residual"),
+        "simpfem_true_residual_noalloc": ((N, N, N, N, N, N, N), "true_residual_noalloc"),
+        "simpfem_gmg_create": ((N, N, o), "gmg_create"),
+        "simpfem_gmg_setup": ((N, N, N, N), "gmg_setup"),
+        "simpfem_gmg_apply": ((N, N, N, N), "gmg_apply"),
+        "simpfem_gmg_cycle_trace": ((N, N, 0, N, 0, N, N, N), "cycle_trace"),
+        "simpfem_gmg_props_get": ((N, N), "props_get"),
+        "simpfem_gmg_reset_lambda_cache": ((N,), "null gmg"),
+        "simpfem_gmg_fine_E": ((N, N), "null argument"),
+        "simpfem_fgmres": ((N, N, N, N, 1e-6, 1, 1, N, 0, N, N, N, N), "simpfem_fgmres"),
+        "simpfem_fgmres_checked": ((N, N, N, N, 1e-6, 1, 1, N, 0, N, N, N, 0, 0, N, N, N, N), "simpfem_fgmres"),
+        "simpfem_pcg": ((N, N, N, N, 1e-6, 1, N, 0, N, N, N, N), "simpfem_pcg"),
+        "simpfem_fgmres_op": ((0, N, N, N, N, N, N, 1e-6, 1, 1, N, 0, N, N, N, N), "simpfem_fgmres_op"),
+        "simpfem_pcg_op": ((0, N, N, N, N, N, N, 1e-6, 1, N, 0, N, N, N, N), "simpfem_pcg_op"),
+        "simpfem_dense_cholesky_inverse": ((-1, N, N, N, N), "dense_cholesky_inverse"),
+        "simpfem_policy_run": ((N, N, N, N, N, N, N), "simpfem_policy"),
+        "simpfem_policy_batch": ((N, N, 0, N, N), "simpfem_policy"),
+        "simpfem_cone_filter": ((0, 0, 0, 1.5, 0, N, N, N), "cone_filter"),
+        "simpfem_oc_update": ((0, N, N, N, N, 0.3, 0.2, N, N, 0, N, N, N, N), "oc_update"),
+        "simpfem_heaviside": ((0, N, 1.0, 0.5, N, N, N), "heaviside"),
+        "simpfem_oc_update_projected": ((0, 0, 0, 1.5, N, N, N, 4.0, 0.5, 0.3, 0.2, N, N, 0, N, N, N, N),
+                                        "oc_update_projected"),
+        "simpfem_cnn_create": ((0, o), "cnn_create"),
+        "simpfem_cnn_set_params": ((N, N, 0), "cnn_set_params"),
+        "simpfem_cnn_get_params": ((N, N, 0), "cnn_get_params"),
+        "simpfem_cnn_pool16": ((0, 0, 0, N, N, N), "cnn_pool16"),
+        "simpfem_cnn_forward": ((N, N, N, 0, N, N), "cnn_forward"),
+        "simpfem_cnn_loss_grad": ((N, N, N, N, 0, N, N, N), "cnn_loss_grad"),
+        "simpfem_cnn_adam_step": ((N, 0.0, 0.0, 0.0, 0.0, N), "cnn_adam_step"),
+    }
+    for name, (args, word) in cases.items():
+        st = getattr(lib, name)(*args)
+        msg = (lib.simpfem_last_error() or b"").decode()
+        assert st == 1 and word in msg, (name, st, msg)
+    for name in ("simpfem_mesh_destroy", "simpfem_gmg_destroy", "simpfem_cnn_destroy"):
+        assert getattr(lib, name)(None) == 0, name
+    status_entries = {n for n, (res, _) in _lib._SIGS.items() if res is ctypes.c_int} - {
+        "simpfem_version", "simpfem_cnn_n_params", "simpfem_mesh_destroy", "simpfem_gmg_destroy",
+        "simpfem_cnn_destroy"}
+    assert status_entries == set(cases), sorted(status_entries ^ set(cases))

@@ -149,7 +149,6 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
                            device: str = "auto", param_controller: Optional[Callable] = None,
                            passive_mask=None, verbose: bool = False, progress_callback: Optional[Callable] = None,
                            solver_class=None, solver_kwargs: Optional[dict] = None) -> dict:
-    torch = _lib.require_cuda()
     t_start = time.time()
     nx, ny, nz = int(params.nelx), int(params.nely), int(params.nelz)
     if nz <= 0:
@@ -159,6 +158,7 @@ def run_simp_surrogate_gpu(params: TO3DParams, fixed, free, F, ndof: int, surrog
     if solver_class is None:
         raise NotImplementedError("the reference's default GPUFEMSolver (assembled CSR) is not provided; "
                                   "pass solver_class=SolverV4 or a subclass")
+    torch = _lib.require_cuda()
     dims = (nx, ny, nz)
     n_elem = nx * ny * nz
     E0, Emin = 1.0, float(params.emin)

@@ -139,3 +139,19 @@ def test_grayness_and_checkerboard_match_reference_definitions():
                  + R[:-1:2, :-1:2, 1::2] + R[1::2, :-1:2, 1::2] + R[:-1:2, 1::2, 1::2] + R[1::2, 1::2, 1::2]) / 8
             ref = float(np.std(b))
         assert abs(_checkerboard(torch.as_tensor(x), *dims) - ref) <= 1e-14, dims
+
+
+def test_entry_refuses_what_it_does_not_provide():
+    """2D meshes, the CPU backend and the reference's default assembled-CSR solver
+    are refused by name, before the device is touched."""
+    import pytest
+
+    from gpu_fem.simp_gpu import TO3DParams, run_simp_surrogate_gpu
+    from gpu_fem.solver_v4 import SolverV4
+
+    with pytest.raises(NotImplementedError, match="3D"):
+        run_simp_surrogate_gpu(TO3DParams(nelz=0), None, None, None, 0, None, None, solver_class=SolverV4)
+    with pytest.raises(NotImplementedError, match="CUDA device"):
+        run_simp_surrogate_gpu(TO3DParams(), None, None, None, 0, None, None, device="cpu", solver_class=SolverV4)
+    with pytest.raises(NotImplementedError, match="GPUFEMSolver"):
+        run_simp_surrogate_gpu(TO3DParams(), None, None, None, 0, None, None)
